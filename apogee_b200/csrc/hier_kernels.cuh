@@ -1,0 +1,137 @@
+// Hierarchical-filter support kernels: FP64 band fractions and coarse
+// template scaling (src/hmf.c:118-156), plus the interface of the tensor-core
+// coarse pass (coarse_tc.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace mfb {
+
+struct HierFpowArgs {
+  const float2 *tmpl;   // [nt][n]
+  int n, m, t0, count;
+  float *fpow;          // [nt]
+};
+struct HierScaleArgs {
+  const float2 *tmpl;   // [nt][n]
+  int n, m, t0, count;
+  int ref_on;
+  float ref_f;
+  const float *fpow;
+  float2 *ct;           // [nt][m]
+};
+
+// Band fraction of each template, sum_{k<m}|H_k|^2 / sum_k |H_k|^2, with both
+// sums in FP64 and the ratio rounded to float (src/hmf.c:144-153).
+static __global__ void hier_fpow_kernel(const HierFpowArgs a) {
+  const int t = a.t0 + blockIdx.x;
+  const float2 *h = a.tmpl + (long long)t * a.n;
+  double low = 0.0, total = 0.0;
+  for (int k = threadIdx.x; k < a.n; k += blockDim.x) {
+    const float2 x = h[k];
+    const double p = (double)x.x * x.x + (double)x.y * x.y;
+    total += p;
+    if (k < a.m) low += p;
+  }
+  __shared__ double sl[32], st[32];
+  for (int o = 16; o; o >>= 1) {
+    low += __shfl_xor_sync(0xffffffffu, low, o);
+    total += __shfl_xor_sync(0xffffffffu, total, o);
+  }
+  if ((threadIdx.x & 31) == 0) { sl[threadIdx.x >> 5] = low; st[threadIdx.x >> 5] = total; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double L = 0.0, S = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { L += sl[w]; S += st[w]; }
+    a.fpow[t] = S > 0.0 ? (float)(L / S) : 0.f;
+  }
+}
+
+// ct[t][k] = (float)(H[t][k] * (1/sqrt(f))) in double, f the reference
+// fraction or the row's own; f <= 0 gives a zero coarse template
+// (src/hmf.c:118-124).
+static __global__ void hier_scale_kernel(const HierScaleArgs a) {
+  const int t = a.t0 + blockIdx.x;
+  const double f = a.ref_on ? (double)a.ref_f : (double)a.fpow[t];
+  const double sc = f > 0.0 ? 1.0 / sqrt(f) : 0.0;
+  const float2 *h = a.tmpl + (long long)t * a.n;
+  float2 *c = a.ct + (long long)t * a.m;
+  for (int k = threadIdx.x; k < a.m; k += blockDim.x) {
+    const float2 x = h[k];
+    c[k] = make_float2((float)((double)x.x * sc), (float)((double)x.y * sc));
+  }
+}
+
+inline cudaError_t launch_hier_fpow(const HierFpowArgs &a, cudaStream_t s) {
+  hier_fpow_kernel<<<a.count, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+inline cudaError_t launch_hier_scale(const HierScaleArgs &a, cudaStream_t s) {
+  hier_scale_kernel<<<a.count, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+static __global__ void reference_sum_kernel(const float *p, int n, int m, double *out) {
+  double low = 0.0, total = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const double x = (double)p[k];
+    total += x;
+    if (k < m) low += x;
+  }
+  __shared__ double sl[32], st[32];
+  for (int o = 16; o; o >>= 1) {
+    low += __shfl_xor_sync(0xffffffffu, low, o);
+    total += __shfl_xor_sync(0xffffffffu, total, o);
+  }
+  if ((threadIdx.x & 31) == 0) { sl[threadIdx.x >> 5] = low; st[threadIdx.x >> 5] = total; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double L = 0.0, S = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { L += sl[w]; S += st[w]; }
+    out[0] = L;
+    out[1] = S;
+  }
+}
+
+// FP64 in-band and total sums of a host reference profile, on the device
+// (src/hmf.c:125-136).  Synchronous; returns a cudaError_t value.
+inline int reference_fraction_fp64(const float *power_host, size_t n, size_t m, double *low,
+                                   double *total, cudaStream_t s) {
+  float *dp = nullptr;
+  double *dout = nullptr;
+  cudaError_t e = cudaMalloc(&dp, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dout, 2 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, power_host, n * sizeof(float), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) { reference_sum_kernel<<<1, 1024, 0, s>>>(dp, (int)n, (int)m, dout); e = cudaGetLastError(); }
+  double h[2] = {0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, dout, sizeof h, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dp);
+  cudaFree(dout);
+  *low = h[0];
+  *total = h[1];
+  return (int)e;
+}
+
+// ---- tensor-core coarse pass (coarse_tc.cu) --------------------------------
+struct TcCoarse;
+struct TcRunArgs {
+  const float2 *data;   // full-length data rows [nd_total][n]; the first m bins are used
+  int n;
+  int d0, nd, t0, nt;
+  int ws, we;           // coarse window [ws, we) on the m-point grid
+  float gate;
+  long long *out_idx;   // full-size outputs: rows of dismissed pairs get (-1, 0)
+  float2 *out_val;
+  int rs;               // record stride of out_idx/out_val in 8-byte units (1 or 2)
+  int full_nb;
+  int32_t *fire_list, *fire_count;
+  float *coarse_out;    // if set: write max |z| per pair here instead of gating
+};
+int tc_coarse_create(TcCoarse **out, int m, int ntmpl, int ndata, int fp16);
+void tc_coarse_destroy(TcCoarse *c);
+int tc_coarse_pack_templates(TcCoarse *c, const float2 *ct, int t0, int count, cudaStream_t s);
+int tc_coarse_run(TcCoarse *c, const TcRunArgs &a, cudaStream_t s);
+const char *tc_coarse_error();
+
+}  // namespace mfb

@@ -1,0 +1,818 @@
+// C ABI of libmfb.so: plans, ingest, launches.  See include/mfb.h.
+//
+// Host-side structure mirrors the reference engine (src/matchfilt.c for the
+// flat plan, src/hmf.c for the hierarchical plan) but every hot loop is a
+// device kernel on the plan's stream; the host only validates arguments and
+// enqueues.  Nothing here allocates on the run path: buffers are sized at
+// creation or grown on first use of a larger shape.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstdarg>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <mutex>
+#include <map>
+#include <algorithm>
+#include "../../include/mfb.h"
+#include "flat_kernel.cuh"
+#include "series_kernel.cuh"
+#include "hier_kernels.cuh"
+
+using namespace mfb;
+
+// ---------------------------------------------------------------- errors
+static thread_local std::string g_err;
+
+static int fail(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+static int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+#define CUDA_TRY(expr)                                                              \
+  do {                                                                              \
+    cudaError_t _e = (expr);                                                        \
+    if (_e != cudaSuccess)                                                          \
+      return fail(MFB_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e),    \
+                  __FILE__, __LINE__);                                              \
+  } while (0)
+
+extern "C" const char *mfb_last_error(void) { return g_err.c_str(); }
+
+// ------------------------------------------------------- twiddle tables
+// exp(+2*pi*i*m/M), from double-precision cos/sin of a first-quadrant angle
+// and an exact quadrant rotation, so that multiples of pi/2 come out as exact
+// 0 and +-1 and the two components of pi/4 are equal.
+static float2 unit_root(long long m, long long M) {
+  m %= M;
+  if (m < 0) m += M;
+  const long long q4 = (4 * m) / M;          // quadrant
+  const long long r = 4 * m - q4 * M;        // remainder, angle = (pi/2) * r / M
+  double c0, s0;
+  if (2 * r <= M) {
+    const double th = M_PI / 2 * (double)r / (double)M;
+    c0 = std::cos(th); s0 = std::sin(th);
+  } else {
+    const double th = M_PI / 2 * (double)(M - r) / (double)M;
+    c0 = std::sin(th); s0 = std::cos(th);
+  }
+  if (r == 0) { c0 = 1.0; s0 = 0.0; }
+  double c, s;
+  switch (q4) {
+    case 0: c = c0; s = s0; break;
+    case 1: c = -s0; s = c0; break;
+    case 2: c = -c0; s = -s0; break;
+    default: c = s0; s = -c0; break;
+  }
+  return make_float2((float)c, (float)s);
+}
+
+template <int N>
+static std::vector<float2> build_twiddles() {
+  std::vector<float2> tw(twiddle_count<N>() > 0 ? twiddle_count<N>() : 1);
+  for (int p = 1; p < FlatGeo<N>::PASSES; p++) {
+    const int Ns = span_before<N>(p);
+    const int off = twiddle_offset<N>(p);
+    for (int q = 1; q < 16; q++)
+      for (int k = 0; k < Ns; k++)
+        tw[off + (q - 1) * Ns + k] = unit_root((long long)q * k, 16LL * Ns);
+  }
+  return tw;
+}
+
+// Per-(device, n) constant state: twiddles and launch shapes.
+struct NConst {
+  float2 *twid = nullptr;
+  int grid_peaks = 0, grid_gate = 0, grid_fwd = 0;
+  int cta = 0, smem = 0, g = 0;
+};
+static std::mutex g_const_mu;
+static std::map<std::pair<int, int>, NConst> g_const;
+
+template <int N>
+static int make_const(int device, NConst &c) {
+  using Geo = FlatGeo<N>;
+  auto tw = build_twiddles<N>();
+  CUDA_TRY(cudaMalloc(&c.twid, tw.size() * sizeof(float2)));
+  CUDA_TRY(cudaMemcpy(c.twid, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  c.cta = Geo::CTA;
+  c.smem = Geo::SMEM;
+  c.g = Geo::G;
+  CUDA_TRY(cudaFuncSetAttribute(flat_kernel<N, MODE_PEAKS>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, Geo::SMEM));
+  CUDA_TRY(cudaFuncSetAttribute(flat_kernel<N, MODE_GATE>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, Geo::SMEM));
+  CUDA_TRY(cudaFuncSetAttribute(series_forward_kernel<N>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, Geo::SMEM));
+  int sms = 0, b1 = 0, b2 = 0, b3 = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, flat_kernel<N, MODE_PEAKS>,
+                                                         Geo::CTA, Geo::SMEM));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, flat_kernel<N, MODE_GATE>,
+                                                         Geo::CTA, Geo::SMEM));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, series_forward_kernel<N>,
+                                                         Geo::CTA, Geo::SMEM));
+  if (b1 < 1 || b2 < 1 || b3 < 1)
+    return fail(MFB_ERR_CUDA, "kernel for n=%d cannot be resident on this device", N);
+  c.grid_peaks = b1 * sms;
+  c.grid_gate = b2 * sms;
+  c.grid_fwd = b3 * sms;
+  return MFB_OK;
+}
+
+static int get_const(int device, int n, NConst **out) {
+  std::lock_guard<std::mutex> lk(g_const_mu);
+  auto key = std::make_pair(device, n);
+  auto it = g_const.find(key);
+  if (it != g_const.end()) { *out = &it->second; return MFB_OK; }
+  NConst c;
+  int r;
+  switch (n) {
+    case 64: r = make_const<64>(device, c); break;
+    case 128: r = make_const<128>(device, c); break;
+    case 256: r = make_const<256>(device, c); break;
+    case 512: r = make_const<512>(device, c); break;
+    case 1024: r = make_const<1024>(device, c); break;
+    case 2048: r = make_const<2048>(device, c); break;
+    case 4096: r = make_const<4096>(device, c); break;
+    case 8192: r = make_const<8192>(device, c); break;
+    case 16384: r = make_const<16384>(device, c); break;
+    default: return fail(MFB_ERR_UNSUPPORTED, "unsupported transform length n=%d", n);
+  }
+  if (r != MFB_OK) return r;
+  *out = &(g_const[key] = c);
+  return MFB_OK;
+}
+
+template <int MODE>
+static cudaError_t launch_flat(int n, const NConst &c, const FlatArgs &a, cudaStream_t s) {
+  const int grid = MODE == MODE_PEAKS ? c.grid_peaks : c.grid_gate;
+  switch (n) {
+#define MFB_CASE(NN) case NN: flat_kernel<NN, MODE><<<grid, c.cta, c.smem, s>>>(a); break;
+    MFB_CASE(64) MFB_CASE(128) MFB_CASE(256) MFB_CASE(512) MFB_CASE(1024)
+    MFB_CASE(2048) MFB_CASE(4096) MFB_CASE(8192) MFB_CASE(16384)
+#undef MFB_CASE
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_forward(int n, const NConst &c, const SeriesArgs &a, cudaStream_t s) {
+  switch (n) {
+#define MFB_CASE(NN) case NN: series_forward_kernel<NN><<<c.grid_fwd, c.cta, c.smem, s>>>(a); break;
+    MFB_CASE(64) MFB_CASE(128) MFB_CASE(256) MFB_CASE(512) MFB_CASE(1024)
+    MFB_CASE(2048) MFB_CASE(4096) MFB_CASE(8192) MFB_CASE(16384)
+#undef MFB_CASE
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+extern "C" int mfb_supported(size_t n) {
+  return n >= 64 && n <= 16384 && (n & (n - 1)) == 0;
+}
+
+extern "C" size_t mfb_nbins(size_t n, size_t binsize, size_t start, size_t end) {
+  if (!binsize) return 0;
+  if (end > n) end = n;
+  if (start >= end) return 0;
+  return (end - start + binsize - 1) / binsize;
+}
+
+// ---------------------------------------------------------------- flat plan
+struct mfb_plan {
+  int device = 0;
+  size_t n = 0;
+  int nd = 0, nt = 0;
+  float2 *data = nullptr;   // [nd][n]
+  float2 *tmpl = nullptr;   // [nt][n]
+  cudaStream_t stream = nullptr;
+  NConst *c = nullptr;
+  // run_series workspace: block starts and block spectra
+  uint64_t *starts_dev = nullptr;
+  int starts_cap = 0;
+  float2 *sspec = nullptr;
+  int sspec_rows = 0;
+};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+extern "C" int mfb_create(mfb_plan **out, size_t n, int ndata, int ntmpl, int device) {
+  if (!out) return fail(MFB_ERR_ARG, "null output handle");
+  *out = nullptr;
+  if (ndata < 1 || ntmpl < 1) return fail(MFB_ERR_ARG, "ndata and ntemplates must be >= 1");
+  if (!mfb_supported(n))
+    return fail(MFB_ERR_UNSUPPORTED,
+                "unsupported matched-filter shape n=%zu ndata=%d ntemplates=%d", n, ndata, ntmpl);
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(MFB_ERR_ARG, "no CUDA device %d", device);
+  DeviceGuard dg(device);
+  mfb_plan *p = new mfb_plan;
+  p->device = device;
+  p->n = n;
+  p->nd = ndata;
+  p->nt = ntmpl;
+  int r = get_const(device, (int)n, &p->c);
+  if (r != MFB_OK) { delete p; return r; }
+  cudaError_t e1 = cudaMalloc(&p->data, (size_t)ndata * n * sizeof(float2));
+  cudaError_t e2 = e1 == cudaSuccess ? cudaMalloc(&p->tmpl, (size_t)ntmpl * n * sizeof(float2)) : e1;
+  if (e2 != cudaSuccess) {
+    cudaFree(p->data);
+    delete p;
+    return fail(MFB_ERR_CUDA, "device allocation of %zu bytes failed: %s",
+                ((size_t)ndata + ntmpl) * n * sizeof(float2), cudaGetErrorString(e2));
+  }
+  // Unset rows are zero spectra, not garbage.
+  cudaMemset(p->data, 0, (size_t)ndata * n * sizeof(float2));
+  cudaMemset(p->tmpl, 0, (size_t)ntmpl * n * sizeof(float2));
+  CUDA_TRY(cudaDeviceSynchronize());
+  *out = p;
+  return MFB_OK;
+}
+
+extern "C" int mfb_destroy(mfb_plan *p) {
+  if (!p) return MFB_OK;
+  DeviceGuard dg(p->device);
+  if (p->stream) cudaStreamSynchronize(p->stream); else cudaDeviceSynchronize();
+  cudaFree(p->data);
+  cudaFree(p->tmpl);
+  cudaFree(p->starts_dev);
+  cudaFree(p->sspec);
+  delete p;
+  return MFB_OK;
+}
+
+extern "C" int mfb_set_stream(mfb_plan *p, void *stream) {
+  if (!p) return fail(MFB_ERR_ARG, "null plan");
+  p->stream = (cudaStream_t)stream;
+  return MFB_OK;
+}
+
+static int copy_rows(float2 *dst, size_t n, int rows, int r0, int count, const void *src,
+                     cudaStream_t s, const char *what) {
+  if (!src) return fail(MFB_ERR_ARG, "null %s spectrum", what);
+  if (count < 1 || r0 < 0 || r0 > rows - count)
+    return fail(MFB_ERR_INDEX, "%s rows [%d, %d) out of range [0, %d)", what, r0, r0 + count, rows);
+  CUDA_TRY(cudaMemcpyAsync(dst + (size_t)r0 * n, src, (size_t)count * n * sizeof(float2),
+                           cudaMemcpyDefault, s));
+  return MFB_OK;
+}
+
+extern "C" int mfb_set_data(mfb_plan *p, int d0, int count, const void *spec) {
+  if (!p) return fail(MFB_ERR_ARG, "null plan");
+  DeviceGuard dg(p->device);
+  return copy_rows(p->data, p->n, p->nd, d0, count, spec, p->stream, "data");
+}
+
+extern "C" int mfb_set_templates(mfb_plan *p, int t0, int count, const void *spec) {
+  if (!p) return fail(MFB_ERR_ARG, "null plan");
+  DeviceGuard dg(p->device);
+  return copy_rows(p->tmpl, p->n, p->nt, t0, count, spec, p->stream, "template");
+}
+
+// Validates a run's block, window and bins exactly as the reference binding
+// does (python/matchedfilter/_core.c:29-43): returns nb or an error code.
+static int check_run(const mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
+                     size_t start, size_t end, size_t *nb) {
+  if (d0 < 0 || nd < 1 || nd > p->nd || d0 > p->nd - nd || t0 < 0 || nt < 1 || nt > p->nt ||
+      t0 > p->nt - nt || binsize < 1 || start >= p->n || end <= start)
+    return fail(MFB_ERR_ARG, "invalid subrange, binsize or window");
+  if (end > p->n) end = p->n;
+  *nb = 1 + (end - start - 1) / binsize;
+  return MFB_OK;
+}
+
+static FlatArgs base_args(const mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
+                          float threshold, size_t start, size_t end, size_t nb) {
+  FlatArgs a;
+  memset(&a, 0, sizeof a);
+  a.data = p->data;
+  a.tmpl = p->tmpl;
+  a.data_stride = (long long)p->n;
+  a.tmpl_stride = (long long)p->n;
+  a.twid = p->c->twid;
+  a.d0 = d0; a.nd = nd; a.t0 = t0; a.nt = nt;
+  if (end > p->n) end = p->n;
+  a.ws = (int)start;
+  a.we = (int)end;
+  a.binsize = binsize > p->n ? (int)p->n : (int)binsize;   // one bin either way
+  a.nb = (int)nb;
+  a.t2 = threshold > 0.f ? threshold * threshold : 0.f;
+  return a;
+}
+
+static int run_impl(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
+                    float threshold, size_t start, size_t end, int64_t *idx, void *val,
+                    int32_t *counts, int rs) {
+  if (!p) return fail(MFB_ERR_ARG, "null plan");
+  size_t nb;
+  int r = check_run(p, d0, nd, t0, nt, binsize, start, end, &nb);
+  if (r) return r;
+  if (!idx || !val) return fail(MFB_ERR_ARG, "null output");
+  if (std::isnan(threshold)) return fail(MFB_ERR_ARG, "threshold is NaN");
+  DeviceGuard dg(p->device);
+  FlatArgs a = base_args(p, d0, nd, t0, nt, binsize, threshold, start, end, nb);
+  a.out_idx = (long long *)idx;
+  a.out_val = (float2 *)val;
+  a.rs = rs;
+  a.out_cnt = counts;
+  if (counts) CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nd * nt * sizeof(int32_t), p->stream));
+  CUDA_TRY(launch_flat<MODE_PEAKS>((int)p->n, *p->c, a, p->stream));
+  return MFB_OK;
+}
+
+extern "C" int mfb_run(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
+                       float threshold, size_t start, size_t end, int64_t *idx, void *val,
+                       int32_t *counts) {
+  return run_impl(p, d0, nd, t0, nt, binsize, threshold, start, end, idx, val, counts, 1);
+}
+
+extern "C" int mfb_run_records(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
+                               float threshold, size_t start, size_t end, void *records,
+                               int32_t *counts) {
+  if (!records) return fail(MFB_ERR_ARG, "null output");
+  return run_impl(p, d0, nd, t0, nt, binsize, threshold, start, end, (int64_t *)records,
+                  (char *)records + 8, counts, 2);
+}
+
+static int run_rows_impl(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *rows,
+                         const int32_t *nrows, int max_rows, size_t binsize, float threshold,
+                         size_t start, size_t end, int64_t *idx, void *val, int32_t *counts,
+                         int rs) {
+  if (!p) return fail(MFB_ERR_ARG, "null plan");
+  size_t nb;
+  int r = check_run(p, d0, nd, t0, nt, binsize, start, end, &nb);
+  if (r) return r;
+  if (!idx || !val || !rows || !nrows) return fail(MFB_ERR_ARG, "null pointer argument");
+  if (max_rows < 0) return fail(MFB_ERR_ARG, "max_rows must be >= 0");
+  DeviceGuard dg(p->device);
+  FlatArgs a = base_args(p, d0, nd, t0, nt, binsize, threshold, start, end, nb);
+  a.list = rows;
+  a.list_count = nrows;
+  a.out_idx = (long long *)idx;
+  a.out_val = (float2 *)val;
+  a.rs = rs;
+  a.out_cnt = counts;   // rows not listed keep whatever the caller put there
+  CUDA_TRY(launch_flat<MODE_PEAKS>((int)p->n, *p->c, a, p->stream));
+  return MFB_OK;
+}
+
+extern "C" int mfb_run_rows(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *rows,
+                            const int32_t *nrows, int max_rows, size_t binsize, float threshold,
+                            size_t start, size_t end, int64_t *idx, void *val, int32_t *counts) {
+  return run_rows_impl(p, d0, nd, t0, nt, rows, nrows, max_rows, binsize, threshold, start, end,
+                       idx, val, counts, 1);
+}
+
+extern "C" int mfb_forward(mfb_plan *p, const void *series, size_t nseries,
+                           const uint64_t *starts_dev, int nblocks, void *spectra) {
+  if (!p) return fail(MFB_ERR_ARG, "null plan");
+  if (!series || !starts_dev || !spectra || nblocks < 1)
+    return fail(MFB_ERR_ARG, "invalid forward-transform arguments");
+  DeviceGuard dg(p->device);
+  SeriesArgs s;
+  s.series = (const float2 *)series;
+  s.nseries = (long long)nseries;
+  s.starts = (const unsigned long long *)starts_dev;
+  s.nblocks = nblocks;
+  s.out = (float2 *)spectra;
+  s.out_stride = (long long)p->n;
+  s.twid = p->c->twid;
+  s.scale = 1.0f / (float)p->n;
+  CUDA_TRY(launch_forward((int)p->n, *p->c, s, p->stream));
+  return MFB_OK;
+}
+
+extern "C" int mfb_run_series(mfb_plan *p, const void *series, size_t nseries,
+                              const uint64_t *starts, const uint64_t *win_start,
+                              const uint64_t *win_end, int nblocks, int t0, int nt,
+                              size_t binsize, float threshold, int64_t *idx, void *val,
+                              int32_t *counts) {
+  if (!p) return fail(MFB_ERR_ARG, "null plan");
+  if (!series || !starts || !win_start || !win_end || nblocks < 1 || !idx || !val)
+    return fail(MFB_ERR_ARG, "invalid run_series arguments");
+  if (t0 < 0 || nt < 1 || t0 > p->nt - nt || binsize < 1)
+    return fail(MFB_ERR_ARG, "invalid template range or binsize");
+  // Every window must give the same bin count (src/matchfilt.c:477-487).
+  size_t nb0 = 0;
+  for (int b = 0; b < nblocks; b++) {
+    size_t lo = win_start[b], hi = win_end[b] > p->n ? p->n : win_end[b];
+    if (lo >= hi || starts[b] > (uint64_t)INT64_MAX - p->n)
+      return fail(MFB_ERR_ARG, "block %d has an empty window or an overflowing start", b);
+    size_t nb = 1 + (hi - lo - 1) / binsize;
+    if (b == 0) nb0 = nb;
+    else if (nb != nb0) return fail(MFB_ERR_ARG, "block windows must have equal bin counts");
+  }
+  DeviceGuard dg(p->device);
+  if (p->starts_cap < nblocks) {
+    cudaFree(p->starts_dev);
+    p->starts_dev = nullptr;
+    p->starts_cap = 0;
+    CUDA_TRY(cudaMalloc(&p->starts_dev, (size_t)nblocks * sizeof(uint64_t)));
+    p->starts_cap = nblocks;
+  }
+  CUDA_TRY(cudaMemcpyAsync(p->starts_dev, starts, (size_t)nblocks * sizeof(uint64_t),
+                           cudaMemcpyHostToDevice, p->stream));
+  if (counts) CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nblocks * nt * sizeof(int32_t), p->stream));
+  // Block spectra go to a workspace of up to 64 MiB (at least one block),
+  // grown on first use; the plan's data rows are left alone.
+  const size_t row_bytes = p->n * sizeof(float2);
+  int cap = (int)std::max<size_t>(1, ((size_t)64 << 20) / row_bytes);
+  if (cap > nblocks) cap = nblocks;
+  if (p->sspec_rows < cap) {
+    cudaFree(p->sspec);
+    p->sspec = nullptr;
+    p->sspec_rows = 0;
+    CUDA_TRY(cudaMalloc(&p->sspec, (size_t)cap * row_bytes));
+    p->sspec_rows = cap;
+  }
+  // Groups of consecutive equal windows, at most `cap` blocks each.
+  for (int b0 = 0; b0 < nblocks;) {
+    int g = 1;
+    while (g < cap && b0 + g < nblocks && win_start[b0 + g] == win_start[b0] &&
+           win_end[b0 + g] == win_end[b0])
+      g++;
+    int r = mfb_forward(p, series, nseries, p->starts_dev + b0, g, p->sspec);
+    if (r) return r;
+    size_t lo = win_start[b0], hi = win_end[b0];
+    FlatArgs a = base_args(p, 0, g, t0, nt, binsize, threshold, lo, hi, nb0);
+    a.data = p->sspec;
+    a.out_idx = (long long *)idx + (size_t)b0 * nt * nb0;
+    a.out_val = (float2 *)val + (size_t)b0 * nt * nb0;
+    a.rs = 1;
+    a.out_cnt = counts ? counts + (size_t)b0 * nt : nullptr;
+    CUDA_TRY(launch_flat<MODE_PEAKS>((int)p->n, *p->c, a, p->stream));
+    b0 += g;
+  }
+  return MFB_OK;
+}
+
+// ---------------------------------------------------------- hierarchical plan
+struct mfb_hplan {
+  int device = 0;
+  size_t n = 0, m = 0;
+  int nd = 0, nt = 0;
+  int kind = MFB_COARSE_FP32;
+  mfb_plan *full = nullptr;     // full-length plan: data and templates at n
+  float2 *ct = nullptr;         // coarse templates [nt][m] = H[:m] / sqrt(f)
+  float *fpow = nullptr;        // per-template band fraction (float, as src/hmf.c:152)
+  unsigned char *tready = nullptr;  // host flags: template row ingested
+  NConst *cc = nullptr;         // constants at length m (FP32 coarse)
+  int ref_on = 0;
+  float ref_f = 0.f;
+  float cal_thr = -1.f;
+  int32_t *fire_list = nullptr; // [nd*nt]
+  int32_t *fire_count = nullptr;// device counter
+  int32_t *fire_host = nullptr; // pinned copy of the last count
+  long long pairs = 0, trig = 0;
+  int pending = 0;              // a run whose trigger count is not yet folded in
+  TcCoarse *tc = nullptr;       // tensor-core coarse state
+};
+
+extern "C" int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, size_t band,
+                               int coarse_kind, int device) {
+  if (!out) return fail(MFB_ERR_ARG, "null output handle");
+  *out = nullptr;
+  if (!mfb_supported(n) || band < 64 || band >= n || (band & (band - 1)))
+    return fail(MFB_ERR_UNSUPPORTED, "no hierarchical plan for n=%zu band=%zu", n, band);
+  if (coarse_kind != MFB_COARSE_FP32 && coarse_kind != MFB_COARSE_BF16X3 &&
+      coarse_kind != MFB_COARSE_FP16X3)
+    return fail(MFB_ERR_ARG, "unknown coarse kind %d", coarse_kind);
+  mfb_plan *full = nullptr;
+  int r = mfb_create(&full, n, ndata, ntmpl, device);
+  if (r) return r;
+  DeviceGuard dg(device);
+  mfb_hplan *h = new mfb_hplan;
+  h->device = device;
+  h->n = n; h->m = band; h->nd = ndata; h->nt = ntmpl; h->kind = coarse_kind;
+  h->full = full;
+  h->tready = (unsigned char *)calloc((size_t)ntmpl, 1);
+  r = get_const(device, (int)band, &h->cc);
+  cudaError_t e = cudaSuccess;
+  if (r == MFB_OK) {
+    e = cudaMalloc(&h->ct, (size_t)ntmpl * band * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMalloc(&h->fpow, (size_t)ntmpl * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&h->fire_list, (size_t)ndata * ntmpl * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&h->fire_count, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMallocHost(&h->fire_host, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(h->ct, 0, (size_t)ntmpl * band * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMemset(h->fpow, 0, (size_t)ntmpl * sizeof(float));
+  }
+  if (r == MFB_OK && e == cudaSuccess && coarse_kind != MFB_COARSE_FP32) {
+    r = tc_coarse_create(&h->tc, (int)band, ntmpl, ndata, coarse_kind == MFB_COARSE_FP16X3);
+    if (r != 0) { r = fail(MFB_ERR_CUDA, "tensor-core coarse setup failed: %s", tc_coarse_error()); }
+  }
+  if (r != MFB_OK || e != cudaSuccess) {
+    if (r == MFB_OK) r = fail(MFB_ERR_CUDA, "hierarchical plan allocation failed: %s",
+                              cudaGetErrorString(e));
+    mfb_hier_destroy(h);
+    return r;
+  }
+  *out = h;
+  return MFB_OK;
+}
+
+extern "C" int mfb_hier_destroy(mfb_hplan *h) {
+  if (!h) return MFB_OK;
+  DeviceGuard dg(h->device);
+  cudaDeviceSynchronize();
+  mfb_destroy(h->full);
+  cudaFree(h->ct);
+  cudaFree(h->fpow);
+  cudaFree(h->fire_list);
+  cudaFree(h->fire_count);
+  cudaFreeHost(h->fire_host);
+  free(h->tready);
+  tc_coarse_destroy(h->tc);
+  delete h;
+  return MFB_OK;
+}
+
+extern "C" int mfb_hier_set_stream(mfb_hplan *h, void *stream) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  return mfb_set_stream(h->full, stream);
+}
+
+extern "C" int mfb_hier_set_data(mfb_hplan *h, int d0, int count, const void *spec) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  return mfb_set_data(h->full, d0, count, spec);
+}
+
+// Rescale coarse templates for rows [t0, t0+count) from the plan's template
+// bank: ct = H[:m] * (1/sqrt(f)) with f the reference fraction or each row's
+// own band fraction (src/hmf.c:118-124,144-156).
+static int refresh_coarse(mfb_hplan *h, int t0, int count) {
+  HierScaleArgs s;
+  s.tmpl = h->full->tmpl;
+  s.n = (int)h->n;
+  s.m = (int)h->m;
+  s.t0 = t0;
+  s.count = count;
+  s.ref_on = h->ref_on;
+  s.ref_f = h->ref_f;
+  s.fpow = h->fpow;
+  s.ct = h->ct;
+  CUDA_TRY(launch_hier_scale(s, h->full->stream));
+  if (h->tc) {
+    int r = tc_coarse_pack_templates(h->tc, h->ct, t0, count, h->full->stream);
+    if (r) return fail(MFB_ERR_CUDA, "tensor-core template pack failed: %s", tc_coarse_error());
+  }
+  return MFB_OK;
+}
+
+extern "C" int mfb_hier_set_templates(mfb_hplan *h, int t0, int count, const void *spec) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  int r = mfb_set_templates(h->full, t0, count, spec);
+  if (r) return r;
+  DeviceGuard dg(h->device);
+  HierFpowArgs f;
+  f.tmpl = h->full->tmpl;
+  f.n = (int)h->n;
+  f.m = (int)h->m;
+  f.t0 = t0;
+  f.count = count;
+  f.fpow = h->fpow;
+  CUDA_TRY(launch_hier_fpow(f, h->full->stream));
+  for (int t = t0; t < t0 + count; t++) h->tready[t] = 1;
+  return refresh_coarse(h, t0, count);
+}
+
+extern "C" int mfb_hier_set_reference(mfb_hplan *h, const float *power) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  DeviceGuard dg(h->device);
+  if (power) {
+    for (size_t k = 0; k < h->n; k++)
+      if (!std::isfinite(power[k]) || power[k] < 0)
+        return fail(MFB_ERR_ARG, "reference must be finite and nonnegative");
+    double low = 0, total = 0;
+    int rr = reference_fraction_fp64(power, h->n, h->m, &low, &total, h->full->stream);
+    if (rr) return fail(MFB_ERR_CUDA, "reference sum failed: %s", cudaGetErrorString((cudaError_t)rr));
+    if (!(total > 0)) return fail(MFB_ERR_ARG, "reference must have positive total power");
+    h->ref_f = (float)(low / total);
+    h->ref_on = 1;
+  } else {
+    h->ref_on = 0;
+  }
+  // Refresh every ingested template (contiguous runs of ready rows).
+  for (int t = 0; t < h->nt;) {
+    if (!h->tready[t]) { t++; continue; }
+    int e = t;
+    while (e < h->nt && h->tready[e]) e++;
+    int r = refresh_coarse(h, t, e - t);
+    if (r) return r;
+    t = e;
+  }
+  return MFB_OK;
+}
+
+extern "C" int mfb_hier_set_threshold(mfb_hplan *h, float thr) {
+  if (!h || !std::isfinite(thr)) return fail(MFB_ERR_ARG, "coarse threshold must be finite");
+  h->cal_thr = thr;
+  return MFB_OK;
+}
+
+// Coarse window on the lag grid R = n/m, widened by one coarse sample
+// (src/hmf.c:233-239).
+static void coarse_window(const mfb_hplan *h, size_t start, size_t end, int *cs, int *ce) {
+  const size_t R = h->n / h->m;
+  size_t cstart = start / R;
+  size_t cend = (end + R - 1) / R;
+  if (cend > h->m) cend = h->m;
+  if (cstart > 0) cstart--;
+  *cs = (int)cstart;
+  *ce = (int)cend;
+}
+
+static void fold_pending(mfb_hplan *h) {
+  if (h->pending) {
+    cudaStreamSynchronize(h->full->stream);
+    h->trig += *h->fire_host;
+    h->pending = 0;
+  }
+}
+
+static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t binsize,
+                         float threshold, size_t start, size_t end, int64_t *idx, void *val,
+                         int32_t *counts, int rs) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  mfb_plan *p = h->full;
+  size_t nb;
+  int r = check_run(p, d0, nd, t0, nt, binsize, start, end, &nb);
+  if (r) return r;
+  if (!idx || !val) return fail(MFB_ERR_ARG, "null output");
+  if (!std::isfinite(h->cal_thr) || h->cal_thr < 0)
+    return fail(MFB_ERR_STATE, "coarse threshold not configured");
+  DeviceGuard dg(h->device);
+  fold_pending(h);
+  if (end > h->n) end = h->n;
+  int cs, ce;
+  coarse_window(h, start, end, &cs, &ce);
+  cudaStream_t s = p->stream;
+  CUDA_TRY(cudaMemsetAsync(h->fire_count, 0, sizeof(int32_t), s));
+  if (counts) CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nd * nt * sizeof(int32_t), s));
+  if (h->kind == MFB_COARSE_FP32) {
+    FlatArgs a;
+    memset(&a, 0, sizeof a);
+    a.data = p->data;
+    a.tmpl = h->ct;
+    a.data_stride = (long long)h->n;   // the first m bins of each full spectrum
+    a.tmpl_stride = (long long)h->m;
+    a.twid = h->cc->twid;
+    a.d0 = d0; a.nd = nd; a.t0 = t0; a.nt = nt;
+    a.ws = cs; a.we = ce; a.binsize = ce - cs; a.nb = 1;
+    a.t2 = h->cal_thr > 0.f ? h->cal_thr * h->cal_thr : 0.f;
+    a.out_idx = (long long *)idx;
+    a.out_val = (float2 *)val;
+    a.rs = rs;
+    a.gate = h->cal_thr;
+    a.fire_list = h->fire_list;
+    a.fire_count = h->fire_count;
+    a.full_nb = (int)nb;
+    CUDA_TRY(launch_flat<MODE_GATE>((int)h->m, *h->cc, a, s));
+  } else {
+    TcRunArgs a;
+    a.data = p->data;
+    a.n = (int)h->n;
+    a.d0 = d0; a.nd = nd; a.t0 = t0; a.nt = nt;
+    a.ws = cs; a.we = ce;
+    a.gate = h->cal_thr;
+    a.out_idx = (long long *)idx;
+    a.out_val = (float2 *)val;
+    a.rs = rs;
+    a.full_nb = (int)nb;
+    a.fire_list = h->fire_list;
+    a.fire_count = h->fire_count;
+    a.coarse_out = nullptr;
+    int rr = tc_coarse_run(h->tc, a, s);
+    if (rr) return fail(MFB_ERR_CUDA, "tensor-core coarse pass failed: %s", tc_coarse_error());
+  }
+  // Refine the survivors with the full filter; no host decision in between.
+  r = run_rows_impl(p, d0, nd, t0, nt, h->fire_list, h->fire_count, nd * nt, binsize, threshold,
+                    start, end, idx, val, counts, rs);
+  if (r) return r;
+  CUDA_TRY(cudaMemcpyAsync(h->fire_host, h->fire_count, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  h->pairs += (long long)nd * nt;
+  h->pending = 1;
+  return MFB_OK;
+}
+
+extern "C" int mfb_hier_run(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t binsize,
+                            float threshold, size_t start, size_t end, int64_t *idx, void *val,
+                            int32_t *counts) {
+  return hier_run_impl(h, d0, nd, t0, nt, binsize, threshold, start, end, idx, val, counts, 1);
+}
+
+extern "C" int mfb_hier_run_records(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t binsize,
+                                    float threshold, size_t start, size_t end, void *records,
+                                    int32_t *counts) {
+  if (!records) return fail(MFB_ERR_ARG, "null output");
+  return hier_run_impl(h, d0, nd, t0, nt, binsize, threshold, start, end, (int64_t *)records,
+                       (char *)records + 8, counts, 2);
+}
+
+extern "C" int mfb_hier_coarse_values(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t start,
+                                      size_t end, float *out) {
+  if (!h || !out) return fail(MFB_ERR_ARG, "null argument");
+  size_t nb;
+  int r = check_run(h->full, d0, nd, t0, nt, 1, start, end, &nb);
+  if (r) return r;
+  DeviceGuard dg(h->device);
+  if (end > h->n) end = h->n;
+  int cs, ce;
+  coarse_window(h, start, end, &cs, &ce);
+  cudaStream_t s = h->full->stream;
+  if (h->kind == MFB_COARSE_FP32) {
+    return fail(MFB_ERR_ARG, "coarse values are reported by the tensor-core coarse kinds");
+  }
+  TcRunArgs a;
+  memset(&a, 0, sizeof a);
+  a.data = h->full->data;
+  a.n = (int)h->n;
+  a.d0 = d0; a.nd = nd; a.t0 = t0; a.nt = nt;
+  a.ws = cs; a.we = ce;
+  a.coarse_out = out;
+  int rr = tc_coarse_run(h->tc, a, s);
+  if (rr) return fail(MFB_ERR_CUDA, "tensor-core coarse pass failed: %s", tc_coarse_error());
+  return MFB_OK;
+}
+
+extern "C" int mfb_hier_last_triggers(mfb_hplan *h, int64_t *triggers) {
+  if (!h || !triggers) return fail(MFB_ERR_ARG, "null argument");
+  DeviceGuard dg(h->device);
+  CUDA_TRY(cudaStreamSynchronize(h->full->stream));
+  *triggers = *h->fire_host;
+  return MFB_OK;
+}
+
+extern "C" int mfb_hier_stats(mfb_hplan *h, int64_t *pairs, int64_t *triggers) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  DeviceGuard dg(h->device);
+  fold_pending(h);
+  if (pairs) *pairs = h->pairs;
+  if (triggers) *triggers = h->trig;
+  return MFB_OK;
+}
+
+extern "C" int mfb_hier_config(mfb_hplan *h, size_t *band, int *kind) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  if (band) *band = h->m;
+  if (kind) *kind = h->kind;
+  return MFB_OK;
+}
+
+// ------------------------------------------------------------ measurement
+__global__ void fp32_fma_probe(float *out, int iters) {
+  float a0 = threadIdx.x * 1e-3f, a1 = a0 + 1.f, a2 = a0 + 2.f, a3 = a0 + 3.f;
+  float a4 = a0 + 4.f, a5 = a0 + 5.f, a6 = a0 + 6.f, a7 = a0 + 7.f;
+  const float b = 0.999999f, c = 1e-7f;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      a0 = fmaf(a0, b, c); a1 = fmaf(a1, b, c); a2 = fmaf(a2, b, c); a3 = fmaf(a3, b, c);
+      a4 = fmaf(a4, b, c); a5 = fmaf(a5, b, c); a6 = fmaf(a6, b, c); a7 = fmaf(a7, b, c);
+    }
+  }
+  const float s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == 12345.f) out[threadIdx.x] = s;   // keeps the loop live
+}
+
+extern "C" int mfb_fp32_peak(int device, double *flops_per_s) {
+  if (!flops_per_s) return fail(MFB_ERR_ARG, "null output");
+  DeviceGuard dg(device);
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  float *out = nullptr;
+  CUDA_TRY(cudaMalloc(&out, 1024 * sizeof(float)));
+  const int threads = 1024, blocks = sms * 2, iters = 4096;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  fp32_fma_probe<<<blocks, threads>>>(out, iters);   // warm-up
+  cudaEventRecord(e0);
+  fp32_fma_probe<<<blocks, threads>>>(out, iters);
+  cudaEventRecord(e1);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (e != cudaSuccess) return fail(MFB_ERR_CUDA, "probe failed: %s", cudaGetErrorString(e));
+  const double fmas = (double)blocks * threads * iters * 16.0 * 8.0;
+  *flops_per_s = 2.0 * fmas / (ms * 1e-3);
+  return MFB_OK;
+}

@@ -1,0 +1,156 @@
+/* mfb.h -- C ABI of the B200 fused matched-filter library (libmfb.so).
+ *
+ * This is the drop-in seam for the device backends of the reference
+ * (ahnitz/Apogee, package `matchedfilter`):
+ *   - the transform backend vtable `ap_backend` (src/backend.h:6-55) and its
+ *     plan wrapper `ap_plan` (src/dispatch.c:17-192), and
+ *   - the GPU context duck-type `Context.peaks / hier_peaks / forward`
+ *     (python/matchedfilter/_vkcompute.py:962,534,855),
+ * behind the same filter-level contract as the reference C API
+ * (python/matchedfilter/matchedfilter.h).  Plain C types only: pointers,
+ * sizes and a CUDA stream passed as void*.
+ *
+ * Conventions (restated from the reference):
+ *   - Correlation z[k] = sum_f D[f] conj(H[f]) exp(+2 pi i f k / n), unnormalised.
+ *   - Bins: nb = ceil((end-start)/binsize) after clamping end to n; bin j covers
+ *     lags [start + j*binsize, min(start + (j+1)*binsize, end)).
+ *   - A bin reports the lag of max |z|^2 iff |z|^2 > threshold^2 (threshold <= 0
+ *     means > 0); otherwise index -1 and value 0.  Exact ties: lowest lag.
+ *   - Output rows: (d-d0)*nt + (t-t0), nb entries per row.
+ *
+ * Memory: spectra are copied into plan-owned device memory at ingest
+ * (source may be host or device memory; cudaMemcpyDefault decides).  Output
+ * pointers (idx, val, counts) are DEVICE pointers.  Runs are asynchronous on
+ * the plan's stream; errors in arguments are reported before anything is
+ * enqueued.
+ *
+ * Return values: 0 (MFB_OK) or a negative MFB_ERR_*; mfb_last_error() gives
+ * the message for the calling thread.  A plan is not safe for concurrent use
+ * from several threads (as src/matchfilt.c plans are not).
+ */
+#ifndef MFB_H
+#define MFB_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MFB_OK               0
+#define MFB_ERR_ARG         -1   /* invalid argument or shape        -> ValueError   */
+#define MFB_ERR_INDEX       -2   /* row index out of range           -> IndexError   */
+#define MFB_ERR_CUDA        -3   /* CUDA runtime failure              -> RuntimeError */
+#define MFB_ERR_UNSUPPORTED -4   /* transform length not implemented  -> ValueError   */
+#define MFB_ERR_STATE       -5   /* plan not ready (e.g. no gate set) -> RuntimeError */
+
+#define MFB_COARSE_FP32   0      /* coarse pass = flat FP32 filter at length band      */
+#define MFB_COARSE_BF16X3 1      /* coarse pass = BF16 hi+lo tensor-core contraction    */
+#define MFB_COARSE_FP16X3 2      /* coarse pass = FP16 hi+lo tensor-core contraction    */
+
+typedef struct mfb_plan mfb_plan;
+typedef struct mfb_hplan mfb_hplan;
+
+/* ---- flat matched filter ------------------------------------------------ */
+
+/* Replaces ap_mf_create (src/matchfilt.c:73-133; matchedfilter.h:53).  n is a
+   power of two, 64..16384; device is a CUDA ordinal.  *out = NULL on error. */
+int mfb_create(mfb_plan **out, size_t n, int ndata, int ntmpl, int device);
+/* Replaces ap_mf_destroy (src/matchfilt.c:135-146). */
+int mfb_destroy(mfb_plan *p);
+/* Stream for every later enqueue on this plan (a cudaStream_t, NULL = legacy). */
+int mfb_set_stream(mfb_plan *p, void *stream);
+/* Replaces ap_mf_set_data / ap_mf_set_template (src/matchfilt.c:179-215):
+   copy `count` spectra of n complex64 (interleaved re,im) into rows d0.. / t0.. */
+int mfb_set_data(mfb_plan *p, int d0, int count, const void *spec);
+int mfb_set_templates(mfb_plan *p, int t0, int count, const void *spec);
+/* Replaces ap_mf_run (src/matchfilt.c:411-420; matchedfilter.h:66-70).
+   idx: int64 [nd*nt*nb]; val: complex64 [nd*nt*nb]; counts: int32 [nd*nt] or NULL. */
+int mfb_run(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize, float threshold,
+            size_t start, size_t end, int64_t *idx, void *val, int32_t *counts);
+/* Same as mfb_run, but the output is one array of 16-byte records laid out
+   as the reference's PEAK_DTYPE = [("index","<i8"),("value","<c8")]
+   (python/matchedfilter/__init__.py:45), so a host copy of it IS the
+   structured result (the assembly of __init__.py:155-173 happens on the
+   device). records: DEVICE [nd*nt*nb] x 16 bytes. */
+int mfb_run_records(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize, float threshold,
+                    size_t start, size_t end, void *records, int32_t *counts);
+/* Replaces ap_mf_run_sel (src/matchfilt.c:492-503) in list form: run only the
+   output rows rows[0..*nrows) of the block [d0,d0+nd) x [t0,t0+nt), where a row
+   is (d-d0)*nt + (t-t0) and the row count lives in DEVICE memory (nrows), so a
+   survivor list made on the GPU needs no host round trip.  max_rows bounds it. */
+int mfb_run_rows(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *rows,
+                 const int32_t *nrows, int max_rows, size_t binsize, float threshold,
+                 size_t start, size_t end, int64_t *idx, void *val, int32_t *counts);
+/* Replaces ap_mf_run_series (src/matchfilt.c:437-490; matchedfilter.h:98-103).
+   series: complex64 [nseries] (device or host); starts/win_start/win_end:
+   host arrays of nblocks.  Every block's window must give the same bin count
+   (MFB_ERR_ARG otherwise).  Block b's spectrum is FFT(series[start..start+n)/n),
+   zero-padded past nseries.  Output [nblocks][nt][nb] in caller order.
+   The plan's data rows are used as scratch: set_data again before run(). */
+int mfb_run_series(mfb_plan *p, const void *series, size_t nseries, const uint64_t *starts,
+                   const uint64_t *win_start, const uint64_t *win_end, int nblocks,
+                   int t0, int nt, size_t binsize, float threshold,
+                   int64_t *idx, void *val, int32_t *counts);
+/* Forward spectra of blocks, FFT(series[start..start+n)/n) zero-padded past
+   nseries, into spectra [nblocks][n] (DEVICE).  Replaces the GPU forward
+   stage Context.forward (python/matchedfilter/_vkcompute.py:855-906). */
+int mfb_forward(mfb_plan *p, const void *series, size_t nseries, const uint64_t *starts_dev,
+                int nblocks, void *spectra);
+/* Replaces ap_mf_nbins / ap_nbins (src/dispatch.c:62-67). */
+size_t mfb_nbins(size_t n, size_t binsize, size_t start, size_t end);
+/* Message of the last error on this thread ("" if none). */
+const char *mfb_last_error(void);
+/* 1 if n is a supported transform length (replaces ap_supported, matchedfilter.h:208). */
+int mfb_supported(size_t n);
+
+/* ---- hierarchical matched filter ----------------------------------------- */
+
+/* Replaces ap_hmf_create_ex (src/hmf.c:33-70): full plan at n plus a coarse
+   pass over the lowest `band` bins (band a power of two, 64 <= band < n). */
+int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, size_t band,
+                    int coarse_kind, int device);
+int mfb_hier_destroy(mfb_hplan *p);
+int mfb_hier_set_stream(mfb_hplan *p, void *stream);
+/* Replaces ap_hmf_set_data / ap_hmf_set_template (src/hmf.c:139-156).  The
+   template's band fraction is summed in FP64 on the device. */
+int mfb_hier_set_data(mfb_hplan *p, int d0, int count, const void *spec);
+int mfb_hier_set_templates(mfb_hplan *p, int t0, int count, const void *spec);
+/* Replaces ap_hmf_set_reference (src/hmf.c:125-138): power is HOST float32[n]
+   or NULL (use each template's own band fraction).  FP64 sums on the device. */
+int mfb_hier_set_reference(mfb_hplan *p, const float *power);
+/* Replaces ap_hmf_set_threshold (src/hmf.c:107-110): finite; negative marks
+   the plan unconfigured and runs then fail with MFB_ERR_STATE. */
+int mfb_hier_set_threshold(mfb_hplan *p, float coarse_threshold);
+/* Replaces ap_hmf_run (src/hmf.c:222-328): coarse pass, gate, and a refine of
+   the survivors with the flat kernel, all enqueued on the stream with no host
+   decision in between.  Same arguments and output as mfb_run. */
+int mfb_hier_run(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t binsize, float threshold,
+                 size_t start, size_t end, int64_t *idx, void *val, int32_t *counts);
+/* mfb_hier_run with PEAK_DTYPE record output, as mfb_run_records. */
+int mfb_hier_run_records(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t binsize,
+                         float threshold, size_t start, size_t end, void *records,
+                         int32_t *counts);
+/* Survivors of the last mfb_hier_run (synchronises the plan's stream). */
+int mfb_hier_last_triggers(mfb_hplan *p, int64_t *triggers);
+/* Replaces ap_hmf_stats (src/hmf.c:84-103): pairs and triggers since creation
+   (synchronises the plan's stream). */
+int mfb_hier_stats(mfb_hplan *p, int64_t *pairs, int64_t *triggers);
+/* Replaces ap_hmf_config (src/hmf.c:104-106). */
+int mfb_hier_config(mfb_hplan *p, size_t *band, int *coarse_kind);
+/* Coarse maxima only (diagnostics and the precision study): for every pair of
+   the block, the maximum |coarse z| over the coarse window, float32 [nd*nt]
+   DEVICE.  Uses the plan's coarse kind. */
+int mfb_hier_coarse_values(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t start,
+                           size_t end, float *out);
+
+/* ---- measurement --------------------------------------------------------- */
+
+/* Measured FP32 FMA throughput of `device` in FLOP/s (2 per FMA), from a
+   register-resident FMA loop over every SM, timed with CUDA events.  The
+   roofline denominator for the FP32 kernels. */
+int mfb_fp32_peak(int device, double *flops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,65 @@
+"""Host-side logic that needs no GPU: layouts, argument checks, device specs."""
+import numpy as np
+import pytest
+
+import apogee_b200 as mf
+from apogee_b200._series import SeriesLayout
+from apogee_b200 import device
+
+
+def test_peak_dtype_is_the_reference_layout():
+    assert mf.PEAK_DTYPE == np.dtype([("index", "<i8"), ("value", "<c8")])
+    assert mf.PEAK_DTYPE.itemsize == 16
+
+
+def test_series_layout_groups_and_restores_order():
+    st = np.array([0, 10, 20, 30, 40], np.int64)
+    lo = np.array([5, 0, 5, 0, 5], np.int64)
+    hi = np.array([50, 45, 50, 45, 50], np.int64)
+    lay = SeriesLayout(64, st, lo, hi, 16).group()
+    assert lay.nbins == 3
+    assert lay.order is not None
+    # grouped windows are contiguous and cover every block once
+    assert sorted(lay.order.tolist()) == list(range(5))
+    spans = [(a, b) for (_, _, a, b) in lay.groups]
+    assert spans[0][0] == 0 and spans[-1][1] == 5
+    assert np.all(lay.starts == st[lay.order])
+
+
+def test_series_layout_refuses_unequal_bin_counts():
+    with pytest.raises(ValueError):
+        SeriesLayout(64, np.zeros(2, np.int64), np.array([0, 0]), np.array([64, 10]), 16)
+    with pytest.raises(ValueError):
+        SeriesLayout(64, np.zeros(1, np.int64), np.array([10]), np.array([10]), 16)
+
+
+def test_series_layout_keeps_adjacent_groups_in_order():
+    st = np.arange(4, dtype=np.int64)
+    lo = np.array([0, 0, 3, 3])
+    hi = np.array([60, 60, 63, 63])
+    lay = SeriesLayout(64, st, lo, hi, 32).group()
+    assert lay.order is None
+    assert [g[2:] for g in lay.groups] == [(0, 2), (2, 4)]
+
+
+def test_device_spec_parsing_without_gpu(monkeypatch):
+    monkeypatch.setattr(device, "devices", lambda: [device.Device(0, "fake"), device.Device(1, "fake")])
+    assert device.parse(None) == "gpu:0"
+    assert device.parse("cuda:1").index == 1
+    assert device.parse("gpu:1") == device.Device(1)
+    with pytest.raises(ValueError):
+        device.parse("cpu")
+    with pytest.raises(ValueError):
+        device.parse("tpu")
+    with pytest.raises(ValueError):
+        device.parse("gpu:7")
+    with pytest.raises(TypeError):
+        device.parse(3)
+    monkeypatch.setenv("MF_DEVICE", "gpu:1")
+    assert device.parse(None).index == 1
+
+
+def test_no_cpu_fallback_without_device(monkeypatch):
+    monkeypatch.setattr(device, "devices", lambda: [])
+    with pytest.raises(RuntimeError):
+        mf.MatchedFilter(4096, 1, 1)
