@@ -547,31 +547,11 @@ class HierarchicalFilter(MatchedFilter):
             _lib.check(_lib.lib().mfb_hier_set_stream(self._hplan, s.cuda_stream))
         return s
 
-    def _ingest(self, fn, spectra, index, rows):
-        # Stage into the device tensors; the plan ingests them at run time.
-        torch = _torch()
-        target = self._gd if rows == self.ndata and fn is _lib.lib().mfb_set_data else self._gt
-        if index is None:
-            s = _Spectra(spectra, (rows, self.n), self.device.index)
-            src = s.keep if _is_torch(s.keep) else torch.from_numpy(s.keep)
-            target.copy_(src)
-        else:
-            s = _Spectra(spectra.reshape(-1) if _is_torch(spectra) else
-                         np.ascontiguousarray(_host_array(spectra), dtype=np.complex64),
-                         (self.n,), self.device.index)
-            src = s.keep if _is_torch(s.keep) else torch.from_numpy(s.keep)
-            target[index].copy_(src)
-        if target is self._gd:
-            self._ddirty = True
-        else:
-            self._tdirty = True
-
     def set_data(self, spectra, index=None):
         index = self._input_index(index, self.ndata)
         torch = _torch()
-        s = _Spectra(spectra, (self.ndata, self.n) if index is None else (self.n,),
-                     self.device.index) if index is None else None
         if index is None:
+            s = _Spectra(spectra, (self.ndata, self.n), self.device.index)
             src = s.keep if _is_torch(s.keep) else torch.from_numpy(s.keep)
             self._gd.copy_(src)
         else:

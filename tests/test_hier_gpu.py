@@ -1,0 +1,150 @@
+"""Hierarchical filter on the device: the one-sided contract
+(python/matchedfilter/__init__.py:1055-1080; tests/test_api.py:163-238)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle, parity
+
+pytestmark = pytest.mark.gpu
+
+
+def _mf():
+    import apogee_b200 as mf
+    return mf
+
+
+def noise(rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+def inspiral_power(n, exponent=-7 / 3.0, knee_frac=0.0150):
+    p = np.zeros(n, dtype=np.float32)
+    k = np.arange(1, n // 2).astype(np.float64)
+    p[1:n // 2] = (k ** exponent / ((knee_frac * n / k) ** 4 + 1.0)).astype(np.float32)
+    return p / p.sum()
+
+
+def template_with_power(n, power):
+    h = np.sqrt(power).astype(np.complex64)
+    return h / np.linalg.norm(h)
+
+
+@pytest.mark.parametrize("coarse", ["fp32"])
+def test_identical_or_absent(coarse):
+    """Every reported peak is bit-identical to the flat filter's; only omissions."""
+    mf = _mf()
+    n, nd, nt = 4096, 4, 4
+    rng = np.random.default_rng(11)
+    power = inspiral_power(n)
+    H = np.stack([template_with_power(n, power) for _ in range(nt)])
+    D = noise(rng, (nd, n))
+    for d in range(nd):
+        lag = 300 + 17 * d
+        D[d] += (12.0 * H[0] * np.exp(2j * np.pi * np.arange(n) * lag / n)).astype(np.complex64)
+    flat = mf.MatchedFilter(n, nd, nt)
+    hf = mf.HierarchicalFilter(n, nd, nt, snr=5.5, fd=1e-2, coarse=coarse)
+    hf.set_reference(power)
+    for o in (flat, hf):
+        o.set_data(D)
+        o.set_templates(H)
+    a = flat.run(binsize=1024, threshold=5.5).copy()
+    b = hf.run(binsize=1024, threshold=5.5)
+    fired = b["index"] >= 0
+    assert fired.any()
+    assert not (fired & (a["index"] < 0)).any()
+    np.testing.assert_array_equal(a["index"][fired], b["index"][fired])
+    np.testing.assert_array_equal(a["value"][fired], b["value"][fired])
+    assert (b["value"][~fired] == 0).all()
+
+
+def test_matches_reference_golden(golden_dir):
+    """Reference hierarchical engine, same inputs, pinned band and gate."""
+    mf = _mf()
+    g = np.load(os.path.join(golden_dir, "hier.npz"))
+    for c in range(int(g["ncases"])):
+        n, nd, nt, band, seed, snr, fd, bs, thr, gate, pairs, trig = g["c%d_par" % c]
+        n, nd, nt, band, bs = int(n), int(nd), int(nt), int(band), int(bs)
+        D, H, P = g["c%d_D" % c], g["c%d_H" % c], g["c%d_power" % c]
+        hf = mf.HierarchicalFilter(n, nd, nt, snr=snr, fd=fd, band=band, coarse="fp32")
+        hf.set_reference(P)
+        hf.set_coarse_threshold(gate)
+        hf.set_data(D)
+        hf.set_templates(H)
+        out = hf.run(binsize=bs, threshold=float(thr))
+        cm = oracle.coarse_max(D, H, band, P)
+        near = np.abs(cm - gate) <= 1e-5 * gate
+        ri = g["c%d_idx" % c]
+        dev_fired = (out["index"] >= 0).any(-1)
+        ref_fired = (ri >= 0).any(-1)
+        assert not ((dev_fired != ref_fired) & ~near).any()
+        z = oracle.correlate(D, H)
+        fired = (cm >= gate) & ~near
+        assert not parity.compare(out["index"], out["value"], z, bs, float(thr), rows_mask=fired)
+        assert hf.stats[0] == nd * nt
+        assert abs(hf.stats[1] - int(trig)) <= near.sum()
+
+
+def test_pure_noise_is_ruled_out():
+    mf = _mf()
+    n, nd = 4096, 64
+    rng = np.random.default_rng(12)
+    power = inspiral_power(n)
+    hf = mf.HierarchicalFilter(n, nd, 1, snr=5.5, fd=1e-2)
+    hf.set_reference(power)
+    hf.set_data(noise(rng, (nd, n)))
+    hf.set_templates(template_with_power(n, power)[None, :])
+    peaks = hf.run(binsize=n, threshold=5.5)
+    assert (peaks["index"] < 0).all()
+    assert hf.refine_rate < 0.25
+
+
+def test_omission_rate_meets_the_budget():
+    """False dismissal at the budget, 1500 trials in one batched run."""
+    mf = _mf()
+    n, trials, snr, fd = 4096, 1500, 5.5, 1e-2
+    rng = np.random.default_rng(13)
+    power = inspiral_power(n)
+    H = template_with_power(n, power)
+    ph = np.exp(2j * np.pi * np.arange(n) / n)
+    D = noise(rng, (trials, n))
+    for i in range(trials):
+        D[i] += (snr * H * ph ** ((37 * i) % n)).astype(np.complex64)
+    flat = mf.MatchedFilter(n, trials, 1)
+    hf = mf.HierarchicalFilter(n, trials, 1, snr=snr, fd=fd)
+    hf.set_reference(power)
+    for o in (flat, hf):
+        o.set_data(D)
+        o.set_templates(H[None, :])
+    a = flat.run(binsize=n, threshold=snr).copy()
+    b = hf.run(binsize=n, threshold=snr)
+    det = a["index"][:, 0, 0] >= 0
+    omitted = det & (b["index"][:, 0, 0] < 0)
+    rate = omitted.sum() / max(det.sum(), 1)
+    assert rate <= 3 * fd, (rate, det.sum())
+
+
+def test_calibration_contract():
+    mf = _mf()
+    n = 1024
+    hf = mf.HierarchicalFilter(n, 1, 1)
+    with pytest.raises(ValueError):
+        hf.set_coarse_threshold(3.0)          # explicit gate needs an explicit band
+    rng = np.random.default_rng(14)
+    hf.set_data(noise(rng, (1, n)))
+    hf.set_templates(noise(rng, (1, n)))
+    with pytest.raises(ValueError):
+        hf.run(binsize=n)                     # no band, no reference
+    hp = mf.HierarchicalFilter(n, 1, 1, band=128)
+    hp.set_data(noise(rng, (1, n)))
+    hp.set_templates(noise(rng, (1, n)))
+    with pytest.raises(ValueError):
+        hp.run(binsize=n)                     # pinned band, no gate and no reference
+    hp.set_coarse_threshold(0.0)              # gate 0: every nonzero pair refines
+    out = hp.run(binsize=256)
+    assert (out["index"] >= 0).all()
+    with pytest.raises(ValueError):
+        mf.HierarchicalFilter(n, 1, 1, band=100)
+    with pytest.raises(ValueError):
+        hp.set_reference(np.zeros(n, np.float32))
