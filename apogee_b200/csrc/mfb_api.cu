@@ -477,9 +477,8 @@ struct mfb_hplan {
   float cal_thr = -1.f;
   int32_t *fire_list = nullptr; // [nd*nt]
   int32_t *fire_count = nullptr;// device counter
-  int32_t *fire_host = nullptr; // pinned copy of the last count
-  long long pairs = 0, trig = 0;
-  int pending = 0;              // a run whose trigger count is not yet folded in
+  unsigned long long *trig_total = nullptr;  // device: survivors summed over runs
+  long long pairs = 0;
   TcCoarse *tc = nullptr;       // tensor-core coarse state
 };
 
@@ -508,7 +507,8 @@ extern "C" int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, 
     if (e == cudaSuccess) e = cudaMalloc(&h->fpow, (size_t)ntmpl * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&h->fire_list, (size_t)ndata * ntmpl * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&h->fire_count, sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMallocHost(&h->fire_host, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&h->trig_total, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(h->trig_total, 0, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(h->ct, 0, (size_t)ntmpl * band * sizeof(float2));
     if (e == cudaSuccess) e = cudaMemset(h->fpow, 0, (size_t)ntmpl * sizeof(float));
   }
@@ -535,7 +535,7 @@ extern "C" int mfb_hier_destroy(mfb_hplan *h) {
   cudaFree(h->fpow);
   cudaFree(h->fire_list);
   cudaFree(h->fire_count);
-  cudaFreeHost(h->fire_host);
+  cudaFree(h->trig_total);
   free(h->tready);
   tc_coarse_destroy(h->tc);
   delete h;
@@ -637,17 +637,13 @@ static void coarse_window(const mfb_hplan *h, size_t start, size_t end, int *cs,
   *ce = (int)cend;
 }
 
-static void fold_pending(mfb_hplan *h) {
-  if (h->pending) {
-    cudaStreamSynchronize(h->full->stream);
-    h->trig += *h->fire_host;
-    h->pending = 0;
-  }
+__global__ void accumulate_triggers(const int32_t *count, unsigned long long *total) {
+  *total += (unsigned long long)*count;
 }
 
 static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t binsize,
                          float threshold, size_t start, size_t end, int64_t *idx, void *val,
-                         int32_t *counts, int rs) {
+                         int32_t *counts, int rs, int phase = 0) {
   if (!h) return fail(MFB_ERR_ARG, "null plan");
   mfb_plan *p = h->full;
   size_t nb;
@@ -657,11 +653,11 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
   if (!std::isfinite(h->cal_thr) || h->cal_thr < 0)
     return fail(MFB_ERR_STATE, "coarse threshold not configured");
   DeviceGuard dg(h->device);
-  fold_pending(h);
   if (end > h->n) end = h->n;
   int cs, ce;
   coarse_window(h, start, end, &cs, &ce);
   cudaStream_t s = p->stream;
+  if (phase != 2) {
   CUDA_TRY(cudaMemsetAsync(h->fire_count, 0, sizeof(int32_t), s));
   if (counts) CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nd * nt * sizeof(int32_t), s));
   if (h->kind == MFB_COARSE_FP32) {
@@ -700,13 +696,15 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
     int rr = tc_coarse_run(h->tc, a, s);
     if (rr) return fail(MFB_ERR_CUDA, "tensor-core coarse pass failed: %s", tc_coarse_error());
   }
+  }
+  if (phase == 1) return MFB_OK;
   // Refine the survivors with the full filter; no host decision in between.
   r = run_rows_impl(p, d0, nd, t0, nt, h->fire_list, h->fire_count, nd * nt, binsize, threshold,
                     start, end, idx, val, counts, rs);
   if (r) return r;
-  CUDA_TRY(cudaMemcpyAsync(h->fire_host, h->fire_count, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  accumulate_triggers<<<1, 1, 0, s>>>(h->fire_count, h->trig_total);
+  CUDA_TRY(cudaGetLastError());
   h->pairs += (long long)nd * nt;
-  h->pending = 1;
   return MFB_OK;
 }
 
@@ -714,6 +712,14 @@ extern "C" int mfb_hier_run(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t
                             float threshold, size_t start, size_t end, int64_t *idx, void *val,
                             int32_t *counts) {
   return hier_run_impl(h, d0, nd, t0, nt, binsize, threshold, start, end, idx, val, counts, 1);
+}
+
+extern "C" int mfb_hier_run_phase(mfb_hplan *h, int phase, int d0, int nd, int t0, int nt,
+                                  size_t binsize, float threshold, size_t start, size_t end,
+                                  int64_t *idx, void *val, int32_t *counts) {
+  if (phase < 0 || phase > 2) return fail(MFB_ERR_ARG, "phase must be 0, 1 or 2");
+  return hier_run_impl(h, d0, nd, t0, nt, binsize, threshold, start, end, idx, val, counts, 1,
+                       phase);
 }
 
 extern "C" int mfb_hier_run_records(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t binsize,
@@ -753,17 +759,21 @@ extern "C" int mfb_hier_coarse_values(mfb_hplan *h, int d0, int nd, int t0, int 
 extern "C" int mfb_hier_last_triggers(mfb_hplan *h, int64_t *triggers) {
   if (!h || !triggers) return fail(MFB_ERR_ARG, "null argument");
   DeviceGuard dg(h->device);
+  int32_t c = 0;
+  CUDA_TRY(cudaMemcpyAsync(&c, h->fire_count, sizeof c, cudaMemcpyDeviceToHost, h->full->stream));
   CUDA_TRY(cudaStreamSynchronize(h->full->stream));
-  *triggers = *h->fire_host;
+  *triggers = c;
   return MFB_OK;
 }
 
 extern "C" int mfb_hier_stats(mfb_hplan *h, int64_t *pairs, int64_t *triggers) {
   if (!h) return fail(MFB_ERR_ARG, "null plan");
   DeviceGuard dg(h->device);
-  fold_pending(h);
+  unsigned long long tot = 0;
+  CUDA_TRY(cudaMemcpyAsync(&tot, h->trig_total, sizeof tot, cudaMemcpyDeviceToHost, h->full->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->full->stream));
   if (pairs) *pairs = h->pairs;
-  if (triggers) *triggers = h->trig;
+  if (triggers) *triggers = (int64_t)tot;
   return MFB_OK;
 }
 

@@ -1,0 +1,84 @@
+"""Seeded synthetic workloads for the benchmark and tests.
+
+No public dataset is involved: these generators stand in for the reference's
+matched-profile inspiral bank (python/matchedfilter/benchmark.py:336;
+tests/test_api.py:26-46) with the shapes and value distributions of the
+benchmark configurations.
+
+Templates: h_k = k^(-7/6) exp(i(2 pi k t_c / n + alpha k^(-5/3))) on bins
+kmin..kmax, zero elsewhere, Hermitian-filled (h_{n-k} = conj(h_k), so the
+time-domain template is real), each normalised to unit L2 over all n bins;
+alpha ~ U[1e2, 1e4], t_c ~ U[0, n).
+
+Data: spectrum of N(0,1) real white noise scaled by 1/sqrt(n), so the
+filter output noise has unit variance and SNR is in units of that sigma
+(the reference's own tests use per-bin complex N(0,1)+iN(0,1) instead,
+tests/test_api.py:53-55).  An injection of template t* at lag tau and SNR A
+adds A * h_{t*} * exp(-2 pi i k tau / n), which peaks at lag tau with value A.
+Both sides are exactly Hermitian: the negative frequencies are written as
+the conjugates of the positive ones.
+"""
+import numpy as np
+
+
+def template_bank(n, nt, rng, kmin=20, kmax=None):
+    kmax = n // 2 - 1 if kmax is None else int(kmax)
+    k = np.arange(kmin, kmax + 1, dtype=np.float64)
+    alpha = rng.uniform(1e2, 1e4, size=(nt, 1))
+    tc = rng.uniform(0, n, size=(nt, 1))
+    half = k ** (-7.0 / 6.0) * np.exp(1j * (2 * np.pi * k * tc / n + alpha * k ** (-5.0 / 3.0)))
+    H = np.zeros((nt, n), np.complex128)
+    H[:, kmin:kmax + 1] = half
+    H[:, n - kmax:n - kmin + 1] = np.conj(half[:, ::-1])
+    H /= np.linalg.norm(H, axis=1, keepdims=True)
+    return H.astype(np.complex64)
+
+
+def noise_spectra(n, nd, rng):
+    """FFT of real N(0,1) noise / sqrt(n), exactly Hermitian."""
+    x = rng.standard_normal((nd, n))
+    half = np.fft.rfft(x, axis=1) / np.sqrt(n)
+    D = np.zeros((nd, n), np.complex128)
+    D[:, :n // 2 + 1] = half
+    D[:, n // 2 + 1:] = np.conj(half[:, 1:n // 2][:, ::-1])
+    D[:, 0] = D[:, 0].real
+    D[:, n // 2] = D[:, n // 2].real
+    return D
+
+
+def inject(D, H, d, t, lag, snr):
+    n = D.shape[1]
+    k = np.arange(n)
+    D[d] += snr * H[t].astype(np.complex128) * np.exp(-2j * np.pi * k * lag / n)
+
+
+def flat_workload(n=4096, nd=16, nt=1024, seed=0, n_injected=2, snr=8.0):
+    """Flat benchmark workload: noise data with `n_injected` segments carrying
+    a random template at a random lag and fixed SNR."""
+    rng = np.random.default_rng(seed)
+    H = template_bank(n, nt, rng)
+    D = noise_spectra(n, nd, rng)
+    inj = []
+    for d in rng.choice(nd, size=n_injected, replace=False):
+        t, lag = int(rng.integers(nt)), int(rng.integers(n))
+        inject(D, H, d, t, lag, snr)
+        inj.append((int(d), t, lag, snr))
+    return D.astype(np.complex64), H, inj
+
+
+def hier_workload(n=4096, nd=16, nt=1024, seed=1, frac=0.10, snr_lo=5.0, snr_hi=12.0):
+    """Hierarchical benchmark workload: noise data, `frac` of the segments
+    carry an injection at SNR U[snr_lo, snr_hi]; the reference profile is the
+    mean |h|^2 over the bank."""
+    rng = np.random.default_rng(seed)
+    H = template_bank(n, nt, rng)
+    D = noise_spectra(n, nd, rng)
+    k = max(1, int(round(frac * nd)))
+    inj = []
+    for d in rng.choice(nd, size=k, replace=False):
+        t, lag = int(rng.integers(nt)), int(rng.integers(n))
+        snr = float(rng.uniform(snr_lo, snr_hi))
+        inject(D, H, d, t, lag, snr)
+        inj.append((int(d), t, lag, snr))
+    power = (np.abs(H.astype(np.complex128)) ** 2).mean(0).astype(np.float32)
+    return D.astype(np.complex64), H, power, inj

@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark: filter pairs/sec at n=4096 -- mixed-precision hierarchical
+filter vs FP32 flat filter, at the same false-dismissal rate.
+
+Workload (one GPU): n=4096, 16 data segments x 1024 templates = 16384 pairs,
+binsize 256 (16 bins), hierarchical band 512 (1/8), snr 5.5, fd 1e-2,
+threshold 5.5, reference profile = mean |h|^2 of the bank; synthetic seeded
+inputs (apogee_b200/synthetic.py), 10% of segments injected at SNR U[5,12].
+With --gpus N each rank filters its own 16 x 1024 block (its own template
+slice), so per-GPU work is fixed (weak scaling) and nothing is exchanged.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0).  `value` is device throughput with inputs
+resident in HBM, timed with CUDA events per step (L2 flushed between steps),
+max over ranks; `e2e` is the same metric through the public API
+(HierarchicalFilter.set_data from host memory + run() returning the numpy
+structured result).  `--impl reference` times the reference's own
+single-threaded CPU engine (built from its sources into oracle/_ref) on the
+same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N, ND, NT, BINSIZE, BAND = 4096, 16, 1024, 256, 512
+SNR, FD, THRESHOLD = 5.5, 1e-2, 5.5
+FLOPS_PER_PAIR = lambda n: 5 * n * int(np.log2(n)) + 9 * n   # the reference's own convention
+METRIC = "filter pairs/sec at n=4096: mixed-precision hier vs FP32 flat, same FD rate"
+WORKLOAD = ("hierarchical n=4096 ndata=16 ntemplates=1024 binsize=256 band=512 snr=5.5 "
+            "fd=1e-2 threshold=5.5, 10% of segments injected at SNR U[5,12]")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--coarse", default=os.environ.get("MFB_COARSE", "fp32"),
+                    choices=["fp32", "bf16x3", "fp16x3"])
+    ap.add_argument("--seed", type=int, default=1)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of this GPU's clocks and throttle reasons."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ reference arm
+def reference_arm(args):
+    """The reference's own CPU engine (oracle/_ref), single-threaded."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    try:
+        from oracle import refcore
+        if not refcore.available():
+            raise RuntimeError("oracle/_ref not built")
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU engine: %s" % e}))
+        return
+    from apogee_b200 import synthetic, gatemodel
+    D, H, power, _ = synthetic.hier_workload(N, ND, NT, seed=args.seed)
+    gate = gatemodel.gate_for(power, N, BAND, SNR, FD)
+    r = refcore.RefHier(N, ND, NT, BAND, gate, reference=power, snr=SNR, fd=FD)
+    r.set_templates(H)
+    for _ in range(args.warmup):
+        r.set_data(D)
+        r.run(binsize=BINSIZE, threshold=THRESHOLD)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r.set_data(D)
+        r.run(binsize=BINSIZE, threshold=THRESHOLD)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = ND * NT / dt
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "pairs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "engine": "reference CPU engine, 1 thread, "
+                   "HierarchicalFilter band=512 with the model gate"},
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": 1, "kind": "reference",
+                         "sample": "the full 16x1024 workload per step, %d steps" % args.steps,
+                         "cpu": cpu_model(), "simd": refcore.core().backend()},
+        "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# --------------------------------------------------------------- our arm
+def cpu_baseline_leg(D, H, power, gate, hier_idx):
+    """Rank 0, N=1: the reference CPU engine on a bounded sample, and the
+    false-dismissal of the device hierarchical result against FP64."""
+    out = {}
+    try:
+        from oracle import refcore, oracle
+    except Exception as e:
+        return {"unavailable": str(e)}, None
+    if refcore.available():
+        r = refcore.RefHier(N, ND, NT, BAND, gate, reference=power, snr=SNR, fd=FD)
+        r.set_templates(H)
+        r.set_data(D)
+        r.run(binsize=BINSIZE, threshold=THRESHOLD)
+        reps, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < 3.0 or reps < 3:
+            r.set_data(D)
+            r.run(binsize=BINSIZE, threshold=THRESHOLD)
+            reps += 1
+        hier_v = reps * ND * NT / (time.perf_counter() - t0)
+        f = refcore.RefFlat(N, ND, NT)
+        f.set_templates(H)
+        f.set_data(D)
+        t0 = time.perf_counter()
+        f.run(binsize=BINSIZE, threshold=THRESHOLD)
+        flat_v = ND * NT / (time.perf_counter() - t0)
+        out = {"value": hier_v, "unit": "pairs/s", "cores": 1, "kind": "reference",
+               "sample": "full 16x1024 hierarchical workload, %d runs (~3 s); flat: 1 run" % reps,
+               "flat_value": flat_v, "cpu": cpu_model(), "simd": refcore.core().backend()}
+    # false dismissal vs the FP64 flat filter
+    det = omit = 0
+    for t0 in range(0, NT, 128):
+        z = oracle.correlate(D, H[t0:t0 + 128])
+        m = np.abs(z).reshape(ND, -1, N // BINSIZE, BINSIZE).max(-1)
+        hit = m > THRESHOLD
+        det += int(hit.sum())
+        omit += int((hit & (hier_idx[:, t0:t0 + 128, :] < 0)).sum())
+    fd = {"fp64_detections": det, "omitted": omit, "rate": omit / det if det else 0.0}
+    return out, fd
+
+
+def our_arm(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    import apogee_b200 as mf
+    from apogee_b200 import synthetic, _lib
+    dev = torch.device("cuda", local)
+    D, H, power, inj = synthetic.hier_workload(N, ND, NT, seed=args.seed + 1000 * rank)
+
+    hf = mf.HierarchicalFilter(N, ND, NT, snr=SNR, fd=FD, band=BAND, device="gpu:%d" % local,
+                               coarse=args.coarse)
+    hf.set_reference(power)
+    hf.set_data(D)
+    hf.set_templates(H)
+    first = hf.run(binsize=BINSIZE, threshold=THRESHOLD).copy()       # calibrates, ingests
+    gate = hf._coarse_value(BAND)
+    flat = mf.MatchedFilter(N, ND, NT, device="gpu:%d" % local)
+    flat.set_data(D)
+    flat.set_templates(H)
+    L = _lib.lib()
+    nb = N // BINSIZE
+    rows = ND * NT
+    idx = torch.empty(rows * nb, dtype=torch.int64, device=dev)
+    val = torch.empty(rows * nb, dtype=torch.complex64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
+
+    def hier_step():
+        _lib.check(L.mfb_hier_run(hf._hplan, 0, ND, 0, NT, BINSIZE, THRESHOLD, 0, N,
+                                  idx.data_ptr(), val.data_ptr(), None))
+
+    def flat_step():
+        _lib.check(L.mfb_run(flat._plan, 0, ND, 0, NT, BINSIZE, THRESHOLD, 0, N,
+                             idx.data_ptr(), val.data_ptr(), None))
+
+    def graph_of(step, bind):
+        s = torch.cuda.Stream(dev)
+        s.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(s):
+            bind()
+            step()                                 # warm, outside capture
+        torch.cuda.current_stream(dev).wait_stream(s)
+        torch.cuda.synchronize(dev)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            bind()
+            step()
+        return g
+
+    g_hier = graph_of(hier_step, hf._bind_stream)
+    g_flat = graph_of(flat_step, flat._bind_stream)
+
+    def timed(g, steps, warm, sampler=None):
+        for _ in range(warm):
+            flush.zero_()
+            g.replay()
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        if sampler:
+            sampler.start()
+        evs = []
+        for _ in range(steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            g.replay()
+            b.record()
+            evs.append((a, b))
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        clk = sampler.stop() if sampler else None
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), clk
+
+    sampler = ClockSampler(local)
+    ms_hier, clocks = timed(g_hier, args.steps, args.warmup, sampler)
+    ms_flat, _ = timed(g_flat, max(3, args.steps // 2), args.warmup)
+    hier_ms_step = ms_hier / args.steps
+    flat_ms_step = ms_flat / max(3, args.steps // 2)
+    value = world * rows / (hier_ms_step * 1e-3)
+    flat_value = world * rows / (flat_ms_step * 1e-3)
+
+    # per-kernel durations of the hierarchical step (coarse+gate, refine)
+    def phase_ms(phase, reps=10):
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            hf._bind_stream()
+            if phase == 2:
+                _lib.check(L.mfb_hier_run_phase(hf._hplan, 1, 0, ND, 0, NT, BINSIZE, THRESHOLD,
+                                                0, N, idx.data_ptr(), val.data_ptr(), None))
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            _lib.check(L.mfb_hier_run_phase(hf._hplan, phase, 0, ND, 0, NT, BINSIZE, THRESHOLD,
+                                            0, N, idx.data_ptr(), val.data_ptr(), None))
+            b.record()
+            torch.cuda.synchronize(dev)
+            tot += a.elapsed_time(b)
+        return tot / reps
+    coarse_ms = phase_ms(1)
+    refine_ms = phase_ms(2)
+    trig = hf.last_refinements
+
+    # end to end through the public API (host buffers both ways)
+    def e2e_step():
+        hf.set_data(D)
+        return hf.run(binsize=BINSIZE, threshold=THRESHOLD)
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * rows * args.steps / float(t.item())
+
+    # flat kernel roofline (FP32), the kernel the refine pass runs
+    peak = __import__("ctypes").c_double()
+    _lib.check(L.mfb_fp32_peak(local, __import__("ctypes").byref(peak)))
+    flat_flops = rows * FLOPS_PER_PAIR(N)
+    flat_achieved = flat_flops / (flat_ms_step * 1e-3) / 1e12
+    coarse_flops = rows * FLOPS_PER_PAIR(BAND)
+    refine_flops = trig * FLOPS_PER_PAIR(N)
+    dominant = "coarse" if coarse_ms >= refine_ms else "refine"
+    dom_flops, dom_ms = (coarse_flops, coarse_ms) if dominant == "coarse" else (refine_flops,
+                                                                                refine_ms)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": hier_ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp32": "f32", "bf16x3": "bf16x3+f32", "fp16x3": "f16x3+f32"}[args.coarse],
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "coarse": args.coarse,
+                       "pairs_per_gpu": rows, "l2": "flushed (256 MiB write) between timed steps",
+                       "timing": "CUDA events per step around a CUDA-graph replay"},
+            "flat": {"value": flat_value, "unit": "pairs/s", "ms_per_step": flat_ms_step},
+            "speedup_hier_vs_flat": value / flat_value,
+            "refine_rate": trig / rows,
+            "kernels_ms": {"coarse_gate": coarse_ms, "refine": refine_ms},
+            "roofline": {"bound": "fp32", "kernel": dominant, "achieved": dom_flops / (dom_ms * 1e-3) / 1e12,
+                         "peak": peak.value / 1e12, "unit": "TFLOP/s",
+                         "frac": dom_flops / (dom_ms * 1e-3) / peak.value, "traffic": None,
+                         "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak)"},
+            "roofline_flat": {"bound": "fp32", "achieved": flat_achieved, "peak": peak.value / 1e12,
+                              "unit": "TFLOP/s", "frac": flat_achieved * 1e12 / peak.value,
+                              "flops_per_pair": FLOPS_PER_PAIR(N),
+                              "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak)"},
+            "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": ND * N * 8,
+                    "d2h_bytes_per_step": rows * nb * 16},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks,
+        }
+        if world == 1:
+            cb, fd = cpu_baseline_leg(D, H, power, gate, first["index"])
+            line["cpu_baseline"] = cb
+            line["false_dismissal"] = fd
+        print(json.dumps(line))
+    del g_hier, g_flat
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -130,10 +130,18 @@ int mfb_hier_run(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t binsize, f
 int mfb_hier_run_records(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t binsize,
                          float threshold, size_t start, size_t end, void *records,
                          int32_t *counts);
+/* mfb_hier_run split for measurement: phase 1 enqueues only the coarse pass
+   and gate (dismissed rows written, survivor list built), phase 2 only the
+   refine of the list phase 1 built; phase 0 is the whole run.  Lets a caller
+   time the two kernels of one run separately with events between them. */
+int mfb_hier_run_phase(mfb_hplan *p, int phase, int d0, int nd, int t0, int nt, size_t binsize,
+                       float threshold, size_t start, size_t end, int64_t *idx, void *val,
+                       int32_t *counts);
 /* Survivors of the last mfb_hier_run (synchronises the plan's stream). */
 int mfb_hier_last_triggers(mfb_hplan *p, int64_t *triggers);
 /* Replaces ap_hmf_stats (src/hmf.c:84-103): pairs and triggers since creation
-   (synchronises the plan's stream). */
+   (synchronises the plan's stream).  Triggers are summed on the device, so
+   runs need no host round trip and can be captured in a CUDA graph. */
 int mfb_hier_stats(mfb_hplan *p, int64_t *pairs, int64_t *triggers);
 /* Replaces ap_hmf_config (src/hmf.c:104-106). */
 int mfb_hier_config(mfb_hplan *p, size_t *band, int *coarse_kind);
