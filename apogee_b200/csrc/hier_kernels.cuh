@@ -117,6 +117,7 @@ inline int reference_fraction_fp64(const float *power_host, size_t n, size_t m, 
 struct TcCoarse;
 struct TcRunArgs {
   const float2 *data;   // full-length data rows [nd_total][n]; the first m bins are used
+  const float2 *ct;     // coarse templates [nt_total][m]
   int n;
   int d0, nd, t0, nt;
   int ws, we;           // coarse window [ws, we) on the m-point grid
@@ -133,5 +134,7 @@ void tc_coarse_destroy(TcCoarse *c);
 int tc_coarse_pack_templates(TcCoarse *c, const float2 *ct, int t0, int count, cudaStream_t s);
 int tc_coarse_run(TcCoarse *c, const TcRunArgs &a, cudaStream_t s);
 const char *tc_coarse_error();
+// 0, or -1 if a run timed out waiting for the tensor cores (synchronous).
+int tc_coarse_check(TcCoarse *c);
 
 }  // namespace mfb

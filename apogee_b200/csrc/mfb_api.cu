@@ -681,7 +681,9 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
     CUDA_TRY(launch_flat<MODE_GATE>((int)h->m, *h->cc, a, s));
   } else {
     TcRunArgs a;
+    memset(&a, 0, sizeof a);
     a.data = p->data;
+    a.ct = h->ct;
     a.n = (int)h->n;
     a.d0 = d0; a.nd = nd; a.t0 = t0; a.nt = nt;
     a.ws = cs; a.we = ce;
@@ -747,6 +749,7 @@ extern "C" int mfb_hier_coarse_values(mfb_hplan *h, int d0, int nd, int t0, int 
   TcRunArgs a;
   memset(&a, 0, sizeof a);
   a.data = h->full->data;
+  a.ct = h->ct;
   a.n = (int)h->n;
   a.d0 = d0; a.nd = nd; a.t0 = t0; a.nt = nt;
   a.ws = cs; a.we = ce;
@@ -762,6 +765,7 @@ extern "C" int mfb_hier_last_triggers(mfb_hplan *h, int64_t *triggers) {
   int32_t c = 0;
   CUDA_TRY(cudaMemcpyAsync(&c, h->fire_count, sizeof c, cudaMemcpyDeviceToHost, h->full->stream));
   CUDA_TRY(cudaStreamSynchronize(h->full->stream));
+  if (tc_coarse_check(h->tc)) return fail(MFB_ERR_CUDA, "%s", tc_coarse_error());
   *triggers = c;
   return MFB_OK;
 }
@@ -772,6 +776,7 @@ extern "C" int mfb_hier_stats(mfb_hplan *h, int64_t *pairs, int64_t *triggers) {
   unsigned long long tot = 0;
   CUDA_TRY(cudaMemcpyAsync(&tot, h->trig_total, sizeof tot, cudaMemcpyDeviceToHost, h->full->stream));
   CUDA_TRY(cudaStreamSynchronize(h->full->stream));
+  if (tc_coarse_check(h->tc)) return fail(MFB_ERR_CUDA, "%s", tc_coarse_error());
   if (pairs) *pairs = h->pairs;
   if (triggers) *triggers = (int64_t)tot;
   return MFB_OK;

@@ -31,7 +31,7 @@ def template_with_power(n, power):
     return h / np.linalg.norm(h)
 
 
-@pytest.mark.parametrize("coarse", ["fp32"])
+@pytest.mark.parametrize("coarse", ["fp32", "bf16x3", "fp16x3"])
 def test_identical_or_absent(coarse):
     """Every reported peak is bit-identical to the flat filter's; only omissions."""
     mf = _mf()
@@ -100,7 +100,8 @@ def test_pure_noise_is_ruled_out():
     assert hf.refine_rate < 0.25
 
 
-def test_omission_rate_meets_the_budget():
+@pytest.mark.parametrize("coarse", ["fp32", "bf16x3"])
+def test_omission_rate_meets_the_budget(coarse):
     """False dismissal at the budget, 1500 trials in one batched run."""
     mf = _mf()
     n, trials, snr, fd = 4096, 1500, 5.5, 1e-2
@@ -112,7 +113,7 @@ def test_omission_rate_meets_the_budget():
     for i in range(trials):
         D[i] += (snr * H * ph ** ((37 * i) % n)).astype(np.complex64)
     flat = mf.MatchedFilter(n, trials, 1)
-    hf = mf.HierarchicalFilter(n, trials, 1, snr=snr, fd=fd)
+    hf = mf.HierarchicalFilter(n, trials, 1, snr=snr, fd=fd, band=512, coarse=coarse)
     hf.set_reference(power)
     for o in (flat, hf):
         o.set_data(D)
@@ -148,3 +149,39 @@ def test_calibration_contract():
         mf.HierarchicalFilter(n, 1, 1, band=100)
     with pytest.raises(ValueError):
         hp.set_reference(np.zeros(n, np.float32))
+
+
+@pytest.mark.parametrize("coarse,tol", [("bf16x3", 6e-5), ("fp16x3", 2e-5)])
+def test_tensor_core_coarse_values_vs_fp64(coarse, tol):
+    """Coarse maxima from the split-precision tensor-core contraction, against
+    the FP64 coarse mirror.  Tolerance is relative to the pair's coarse
+    scale (the largest |coarse z|): hi+lo BF16 keeps ~16 bits, FP16 ~22."""
+    mf = _mf()
+    from apogee_b200 import synthetic
+    n, nd, nt, band = 4096, 5, 37, 512
+    D, H, power, _ = synthetic.hier_workload(n, nd, nt, seed=5, frac=0.4)
+    hf = mf.HierarchicalFilter(n, nd, nt, band=band, coarse=coarse)
+    hf.set_reference(power)
+    hf.set_coarse_threshold(1.0)
+    hf.set_data(D)
+    hf.set_templates(H)
+    for window in (None, (100, 4000), (1234, 1300)):
+        got = hf.coarse_values(window=window)
+        want = oracle.coarse_max(D, H, band, power, window)
+        err = np.abs(got - want) / np.maximum(want, 1e-30)
+        assert err.max() < tol, (window, err.max())
+
+
+def test_tensor_core_coarse_tail_pairs():
+    """Pair counts that are not a multiple of the 8-pair tile."""
+    mf = _mf()
+    n, nd, nt, band = 4096, 3, 5, 512
+    rng = np.random.default_rng(15)
+    D, H = noise(rng, (nd, n)), noise(rng, (nt, n))
+    hf = mf.HierarchicalFilter(n, nd, nt, band=band, coarse="bf16x3")
+    hf.set_coarse_threshold(1.0)
+    hf.set_data(D)
+    hf.set_templates(H)
+    got = hf.coarse_values()
+    want = oracle.coarse_max(D, H, band)
+    assert np.abs(got - want).max() < 1e-4 * want.max()
