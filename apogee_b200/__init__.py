@@ -652,6 +652,79 @@ class HierarchicalFilter(MatchedFilter):
         self._cal_thr = value
         self._thr_applied = False
 
+    def calibrate(self, snr=None, fd=None, segments=8192, templates=128, noise="real",
+                  seed=20261203):
+        """Measure the coarse threshold for (snr, fd) on the device and pin it.
+
+        The reference's gate model (gatemodel.gate_for) assumes complex filter
+        output with Re and Im each of unit variance; data whose output noise is
+        distributed differently (real-valued output from Hermitian spectra, for
+        instance) gets a gate that is right for the model, not for the data.
+        This measures the same quantity the model computes -- the fd-quantile
+        of the coarse maximum over pairs whose full filter reaches `snr` --
+        from signals injected at `snr` into independent noise, with this
+        filter's own coarse pass and the flat filter as the fine stage.
+
+        noise: "real" (spectrum of real N(0,1) noise / sqrt(n), Hermitian) or
+        "complex" (per-bin complex normal, unit output variance).  A sample of
+        `templates` templates of the bank is used, `segments` noise segments,
+        one injection each at a uniformly random lag.  Needs a pinned band.
+        Returns the threshold, which is also applied.
+        """
+        if self._pinned is None:
+            raise ValueError("calibrate() needs an explicit band")
+        if self._template_ready is not None:
+            raise ValueError("calibrate() needs the template bank: call set_templates() first")
+        snr = self.snr if snr is None else float(snr)
+        fd = self.fd if fd is None else float(fd)
+        if not (np.isfinite(snr) and snr > 0 and np.isfinite(fd) and 0 < fd < 1):
+            raise ValueError("snr must be positive and fd in (0, 1)")
+        from . import synthetic
+        band, n = self._pinned[0], self.n
+        rng = np.random.default_rng(seed)
+        k = min(int(templates), self.ntemplates)
+        tsel = np.sort(rng.choice(self.ntemplates, size=k, replace=False))
+        Hs = self._gt[tsel].cpu().numpy()
+        kind = {_lib.COARSE_FP32: "fp32", _lib.COARSE_BF16X3: "bf16x3",
+                _lib.COARSE_FP16X3: "fp16x3"}[self._kind]
+        chunk = 512
+        kept = []
+        flat = MatchedFilter(n, chunk, k, device=self.device)
+        coarse = HierarchicalFilter(n, chunk, k, band=band, device=self.device, coarse=kind)
+        coarse.set_coarse_threshold(0.0)
+        flat.set_templates(Hs)
+        coarse.set_templates(Hs)
+        if self._pending_ref is not None:
+            coarse.set_reference(self._pending_ref)
+        ph = np.arange(n)
+        for c0 in range(0, int(segments), chunk):
+            if noise == "real":
+                D = synthetic.noise_spectra(n, chunk, rng)
+            elif noise == "complex":
+                D = (rng.standard_normal((chunk, n)) + 1j * rng.standard_normal((chunk, n))) \
+                    / np.sqrt(2)
+            else:
+                raise ValueError("noise must be 'real' or 'complex'")
+            inj = rng.integers(0, k, size=chunk)
+            lag = rng.integers(0, n, size=chunk)
+            D += snr * Hs[inj].astype(np.complex128) * np.exp(-2j * np.pi * np.outer(lag, ph) / n)
+            D = D.astype(np.complex64)
+            flat.set_data(D)
+            coarse.set_data(D)
+            det = flat.run(binsize=n, threshold=snr)["index"][:, :, 0] >= 0
+            cv = coarse.coarse_values()
+            kept.append(cv[det])
+        kept = np.sort(np.concatenate(kept))
+        i = int(np.floor(fd * kept.size))
+        if i < 8:
+            raise ValueError("too few detections (%d) to place fd=%g; raise segments"
+                             % (kept.size, fd))
+        gate = float(kept[i])
+        self.set_coarse_threshold(gate)
+        self.calibration = {"gate": gate, "detections": int(kept.size), "snr": snr, "fd": fd,
+                            "noise": noise, "segments": int(segments), "templates": k}
+        return gate
+
     def set_first_stage(self, snr):
         """Calibrate the coarse gate at ``snr`` instead of the constructor's."""
         self._fs_snr = float(snr) if snr is not None and float(snr) > 0 else None

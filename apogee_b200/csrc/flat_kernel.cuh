@@ -58,6 +58,7 @@ struct FlatArgs {
   int32_t *fire_list;         // appended output rows that fired
   int32_t *fire_count;        // device counter (zeroed before the launch)
   int full_nb;                // bins of the full-size output written as (-1,0) when dismissed
+  float *coarse_out;          // if set: write max |z| over the window per row instead of gating
 };
 
 template <int N>
@@ -109,7 +110,9 @@ __device__ __forceinline__ int bin_floor(int x, int bs) {
 }
 
 __device__ __forceinline__ void group_sync(int T) {
-  if (T >= 32) __syncthreads(); else __syncwarp();
+  // A pair slot of at most one warp only needs the warp itself in step:
+  // every shared-memory region the kernel uses belongs to one slot.
+  if (T > 32) __syncthreads(); else __syncwarp();
 }
 
 // Unnormalised inverse FFT of the n values x[t + T*s] = v[s] held by the T
@@ -437,7 +440,9 @@ flat_kernel(const FlatArgs a) {
         const unsigned long long kk = keys[0];
         const float m2 = __uint_as_float((unsigned)(kk >> 32));
         const bool fire = kk != 0ull && sqrtf(m2) >= a.gate;
-        if (fire) {
+        if (a.coarse_out) {
+          if (t == 0) a.coarse_out[row] = kk != 0ull ? sqrtf(m2) : 0.f;
+        } else if (fire) {
           if (t == 0) a.fire_list[atomicAdd(a.fire_count, 1)] = row;
         } else {
           const long long obase = (long long)row * a.full_nb;

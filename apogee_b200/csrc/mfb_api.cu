@@ -744,7 +744,19 @@ extern "C" int mfb_hier_coarse_values(mfb_hplan *h, int d0, int nd, int t0, int 
   coarse_window(h, start, end, &cs, &ce);
   cudaStream_t s = h->full->stream;
   if (h->kind == MFB_COARSE_FP32) {
-    return fail(MFB_ERR_ARG, "coarse values are reported by the tensor-core coarse kinds");
+    FlatArgs a;
+    memset(&a, 0, sizeof a);
+    a.data = h->full->data;
+    a.tmpl = h->ct;
+    a.data_stride = (long long)h->n;
+    a.tmpl_stride = (long long)h->m;
+    a.twid = h->cc->twid;
+    a.d0 = d0; a.nd = nd; a.t0 = t0; a.nt = nt;
+    a.ws = cs; a.we = ce; a.binsize = ce - cs; a.nb = 1;
+    a.t2 = 0.f;
+    a.coarse_out = out;
+    CUDA_TRY(launch_flat<MODE_GATE>((int)h->m, *h->cc, a, s));
+    return MFB_OK;
   }
   TcRunArgs a;
   memset(&a, 0, sizeof a);

@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--coarse", default=os.environ.get("MFB_COARSE", "fp32"),
+    ap.add_argument("--coarse", default=os.environ.get("MFB_COARSE", "bf16x3"),
                     choices=["fp32", "bf16x3", "fp16x3"])
     ap.add_argument("--seed", type=int, default=1)
     return ap.parse_args()
@@ -186,15 +186,19 @@ def cpu_baseline_leg(D, H, power, gate, hier_idx):
         out = {"value": hier_v, "unit": "pairs/s", "cores": 1, "kind": "reference",
                "sample": "full 16x1024 hierarchical workload, %d runs (~3 s); flat: 1 run" % reps,
                "flat_value": flat_v, "cpu": cpu_model(), "simd": refcore.core().backend()}
-    # false dismissal vs the FP64 flat filter
-    det = omit = 0
+    # false dismissal vs the FP64 flat filter, for each hierarchical result
+    det = 0
+    omit = {k: 0 for k in hier_idx}
     for t0 in range(0, NT, 128):
         z = oracle.correlate(D, H[t0:t0 + 128])
         m = np.abs(z).reshape(ND, -1, N // BINSIZE, BINSIZE).max(-1)
         hit = m > THRESHOLD
         det += int(hit.sum())
-        omit += int((hit & (hier_idx[:, t0:t0 + 128, :] < 0)).sum())
-    fd = {"fp64_detections": det, "omitted": omit, "rate": omit / det if det else 0.0}
+        for k, hidx in hier_idx.items():
+            omit[k] += int((hit & (hidx[:, t0:t0 + 128, :] < 0)).sum())
+    fd = {"fp64_detections": det}
+    for k in hier_idx:
+        fd[k] = {"omitted": omit[k], "rate": omit[k] / det if det else 0.0}
     return out, fd
 
 
@@ -209,19 +213,30 @@ def our_arm(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+    import ctypes
     import apogee_b200 as mf
     from apogee_b200 import synthetic, _lib
     dev = torch.device("cuda", local)
     D, H, power, inj = synthetic.hier_workload(N, ND, NT, seed=args.seed + 1000 * rank)
+    gdev = "gpu:%d" % local
 
-    hf = mf.HierarchicalFilter(N, ND, NT, snr=SNR, fd=FD, band=BAND, device="gpu:%d" % local,
-                               coarse=args.coarse)
-    hf.set_reference(power)
-    hf.set_data(D)
-    hf.set_templates(H)
-    first = hf.run(binsize=BINSIZE, threshold=THRESHOLD).copy()       # calibrates, ingests
-    gate = hf._coarse_value(BAND)
-    flat = mf.MatchedFilter(N, ND, NT, device="gpu:%d" % local)
+    def make_hier(calibrated):
+        hf = mf.HierarchicalFilter(N, ND, NT, snr=SNR, fd=FD, band=BAND, device=gdev,
+                                   coarse=args.coarse)
+        hf.set_reference(power)
+        hf.set_templates(H)
+        if calibrated:
+            # independent noise and injections (its own seed), device filters only
+            hf.calibrate(snr=SNR, fd=FD, noise="real")
+        hf.set_data(D)
+        return hf
+
+    hf_cal = make_hier(True)
+    hf_mod = make_hier(False)
+    first_cal = hf_cal.run(binsize=BINSIZE, threshold=THRESHOLD).copy()
+    first_mod = hf_mod.run(binsize=BINSIZE, threshold=THRESHOLD).copy()
+    gate_model = hf_mod._coarse_value(BAND)
+    flat = mf.MatchedFilter(N, ND, NT, device=gdev)
     flat.set_data(D)
     flat.set_templates(H)
     L = _lib.lib()
@@ -231,7 +246,7 @@ def our_arm(args):
     val = torch.empty(rows * nb, dtype=torch.complex64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
 
-    def hier_step():
+    def hier_step(hf):
         _lib.check(L.mfb_hier_run(hf._hplan, 0, ND, 0, NT, BINSIZE, THRESHOLD, 0, N,
                                   idx.data_ptr(), val.data_ptr(), None))
 
@@ -253,7 +268,8 @@ def our_arm(args):
             step()
         return g
 
-    g_hier = graph_of(hier_step, hf._bind_stream)
+    g_cal = graph_of(lambda: hier_step(hf_cal), hf_cal._bind_stream)
+    g_mod = graph_of(lambda: hier_step(hf_mod), hf_mod._bind_stream)
     g_flat = graph_of(flat_step, flat._bind_stream)
 
     def timed(g, steps, warm, sampler=None):
@@ -264,7 +280,13 @@ def our_arm(args):
         if world > 1:
             dist.barrier()
         if sampler:
+            # sustained load so that the clock samples see the GPU busy
             sampler.start()
+            t_end = time.perf_counter() + 1.5
+            while time.perf_counter() < t_end:
+                for _ in range(50):
+                    g.replay()
+                torch.cuda.synchronize(dev)
         evs = []
         for _ in range(steps):
             flush.zero_()
@@ -285,15 +307,19 @@ def our_arm(args):
         return float(t.item()), clk
 
     sampler = ClockSampler(local)
-    ms_hier, clocks = timed(g_hier, args.steps, args.warmup, sampler)
-    ms_flat, _ = timed(g_flat, max(3, args.steps // 2), args.warmup)
-    hier_ms_step = ms_hier / args.steps
-    flat_ms_step = ms_flat / max(3, args.steps // 2)
+    ms_cal, clocks = timed(g_cal, args.steps, args.warmup, sampler)
+    ms_mod, _ = timed(g_mod, args.steps, args.warmup)
+    flat_steps = max(3, args.steps // 2)
+    ms_flat, _ = timed(g_flat, flat_steps, args.warmup)
+    hier_ms_step = ms_cal / args.steps
+    model_ms_step = ms_mod / args.steps
+    flat_ms_step = ms_flat / flat_steps
     value = world * rows / (hier_ms_step * 1e-3)
+    model_value = world * rows / (model_ms_step * 1e-3)
     flat_value = world * rows / (flat_ms_step * 1e-3)
 
     # per-kernel durations of the hierarchical step (coarse+gate, refine)
-    def phase_ms(phase, reps=10):
+    def phase_ms(hf, phase, reps=10):
         tot = 0.0
         for _ in range(reps):
             flush.zero_()
@@ -310,14 +336,16 @@ def our_arm(args):
             torch.cuda.synchronize(dev)
             tot += a.elapsed_time(b)
         return tot / reps
-    coarse_ms = phase_ms(1)
-    refine_ms = phase_ms(2)
-    trig = hf.last_refinements
+    coarse_ms = phase_ms(hf_cal, 1)
+    refine_ms = phase_ms(hf_cal, 2)
+    trig = hf_cal.last_refinements
+    phase_ms(hf_mod, 1, 1)
+    trig_mod = hf_mod.last_refinements
 
     # end to end through the public API (host buffers both ways)
     def e2e_step():
-        hf.set_data(D)
-        return hf.run(binsize=BINSIZE, threshold=THRESHOLD)
+        hf_cal.set_data(D)
+        return hf_cal.run(binsize=BINSIZE, threshold=THRESHOLD)
     for _ in range(args.warmup):
         e2e_step()
     torch.cuda.synchronize(dev)
@@ -332,11 +360,11 @@ def our_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * rows * args.steps / float(t.item())
 
-    # flat kernel roofline (FP32), the kernel the refine pass runs
-    peak = __import__("ctypes").c_double()
-    _lib.check(L.mfb_fp32_peak(local, __import__("ctypes").byref(peak)))
+    peak = ctypes.c_double()
+    _lib.check(L.mfb_fp32_peak(local, ctypes.byref(peak)))
     flat_flops = rows * FLOPS_PER_PAIR(N)
     flat_achieved = flat_flops / (flat_ms_step * 1e-3) / 1e12
+    # coarse kernel: the reference's algorithmic flops of a band-point filter per pair
     coarse_flops = rows * FLOPS_PER_PAIR(BAND)
     refine_flops = trig * FLOPS_PER_PAIR(N)
     dominant = "coarse" if coarse_ms >= refine_ms else "refine"
@@ -350,18 +378,26 @@ def our_arm(args):
             "dtype": {"fp32": "f32", "bf16x3": "bf16x3+f32", "fp16x3": "f16x3+f32"}[args.coarse],
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "coarse": args.coarse,
+                       "gate": "calibrated on the device at snr=5.5, fd=1e-2 from independent "
+                               "noise (HierarchicalFilter.calibrate)",
+                       "gate_value": hf_cal.calibration["gate"],
                        "pairs_per_gpu": rows, "l2": "flushed (256 MiB write) between timed steps",
                        "timing": "CUDA events per step around a CUDA-graph replay"},
             "flat": {"value": flat_value, "unit": "pairs/s", "ms_per_step": flat_ms_step},
             "speedup_hier_vs_flat": value / flat_value,
             "refine_rate": trig / rows,
+            "model_gate": {"gate_value": gate_model, "value": model_value,
+                           "ms_per_step": model_ms_step, "refine_rate": trig_mod / rows,
+                           "speedup_vs_flat": model_value / flat_value},
             "kernels_ms": {"coarse_gate": coarse_ms, "refine": refine_ms},
-            "roofline": {"bound": "fp32", "kernel": dominant, "achieved": dom_flops / (dom_ms * 1e-3) / 1e12,
+            "roofline": {"bound": "fp32", "kernel": dominant,
+                         "achieved": dom_flops / (dom_ms * 1e-3) / 1e12,
                          "peak": peak.value / 1e12, "unit": "TFLOP/s",
                          "frac": dom_flops / (dom_ms * 1e-3) / peak.value, "traffic": None,
                          "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak)"},
-            "roofline_flat": {"bound": "fp32", "achieved": flat_achieved, "peak": peak.value / 1e12,
-                              "unit": "TFLOP/s", "frac": flat_achieved * 1e12 / peak.value,
+            "roofline_flat": {"bound": "fp32", "achieved": flat_achieved,
+                              "peak": peak.value / 1e12, "unit": "TFLOP/s",
+                              "frac": flat_achieved * 1e12 / peak.value,
                               "flops_per_pair": FLOPS_PER_PAIR(N),
                               "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak)"},
             "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": ND * N * 8,
@@ -370,11 +406,13 @@ def our_arm(args):
             "clocks": clocks,
         }
         if world == 1:
-            cb, fd = cpu_baseline_leg(D, H, power, gate, first["index"])
+            cb, fd = cpu_baseline_leg(D, H, power, gate_model,
+                                      {"calibrated": first_cal["index"],
+                                       "model": first_mod["index"]})
             line["cpu_baseline"] = cb
             line["false_dismissal"] = fd
         print(json.dumps(line))
-    del g_hier, g_flat
+    del g_cal, g_mod, g_flat
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

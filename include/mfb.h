@@ -145,9 +145,10 @@ int mfb_hier_last_triggers(mfb_hplan *p, int64_t *triggers);
 int mfb_hier_stats(mfb_hplan *p, int64_t *pairs, int64_t *triggers);
 /* Replaces ap_hmf_config (src/hmf.c:104-106). */
 int mfb_hier_config(mfb_hplan *p, size_t *band, int *coarse_kind);
-/* Coarse maxima only (diagnostics and the precision study): for every pair of
-   the block, the maximum |coarse z| over the coarse window, float32 [nd*nt]
-   DEVICE.  Uses the plan's coarse kind. */
+/* Coarse maxima only (gate calibration, diagnostics, the precision study):
+   for every pair of the block, the maximum |coarse z| over the coarse
+   window, float32 [nd*nt] DEVICE (0 where every coarse sample is 0).  Uses
+   the plan's coarse kind. */
 int mfb_hier_coarse_values(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t start,
                            size_t end, float *out);
 
