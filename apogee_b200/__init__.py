@@ -36,7 +36,7 @@ __version__ = "0.1.0"
 PEAK_DTYPE = np.dtype([("index", "<i8"), ("value", "<c8")])
 
 #: Transform lengths the device kernels cover.
-SIZES = frozenset(1 << k for k in range(6, 15))
+SIZES = frozenset(1 << k for k in range(6, 21))
 
 __all__ = ["MatchedFilter", "HierarchicalFilter", "PEAK_DTYPE", "devices", "Device",
            "UnsupportedSize", "backend", "targets", "set_target", "__version__"]

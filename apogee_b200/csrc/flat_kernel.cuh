@@ -115,12 +115,19 @@ __device__ __forceinline__ void group_sync(int T) {
   if (T > 32) __syncthreads(); else __syncwarp();
 }
 
+// Synchronise a pair slot, or the whole CTA when the slot's threads are
+// spread across warps (the column transforms of the large-n kernels).
+template <bool CTA_SYNC>
+__device__ __forceinline__ void pass_sync(int T) {
+  if constexpr (CTA_SYNC) __syncthreads(); else group_sync(T);
+}
+
 // Unnormalised inverse FFT of the n values x[t + T*s] = v[s] held by the T
 // threads of one pair slot (Stockham autosort: pass 0 radix R0, then radix
 // 16).  On return v[q] = X[t + T*q].  buf is this slot's padded shared buffer;
 // the function synchronises the slot before its first store, so buf may
 // still be in use by the caller on entry, and it is free again on return.
-template <int N>
+template <int N, bool CTA_SYNC = false>
 __device__ __forceinline__ void inverse_passes(cf *v, float2 *buf, const float2 *twid, int t) {
   using Geo = FlatGeo<N>;
   constexpr int T = Geo::T, R0 = Geo::R0, PASSES = Geo::PASSES;
@@ -141,7 +148,7 @@ __device__ __forceinline__ void inverse_passes(cf *v, float2 *buf, const float2 
       }
     }
   }
-  group_sync(T);
+  pass_sync<CTA_SYNC>(T);
   // Pass 0 output j*R0 + q (j = t + T*b, q < R0): R0 divides 16, so the
   // 16-block of t*R0 holds every q, and T*R0 is a multiple of 16.
   {
@@ -154,7 +161,7 @@ __device__ __forceinline__ void inverse_passes(cf *v, float2 *buf, const float2 
         p0[q + b * (T * R0 + T * R0 / 16)] = make_float2(x.x, x.y);
       }
   }
-  group_sync(T);
+  pass_sync<CTA_SYNC>(T);
 #pragma unroll
   for (int p = 1; p < PASSES; p++) {
     const int Ns = span_before<N>(p);
@@ -180,7 +187,7 @@ __device__ __forceinline__ void inverse_passes(cf *v, float2 *buf, const float2 
       v[q] = cmul(v[q], cf{w.x, w.y});
     }
     dftR<16, 0, 1>(v);
-    group_sync(T);
+    pass_sync<CTA_SYNC>(T);
     if (p < PASSES - 1) {
       const int base = (t / Ns) * Ns * 16 + k;
       if (Ns % 16 == 0) {
@@ -191,7 +198,7 @@ __device__ __forceinline__ void inverse_passes(cf *v, float2 *buf, const float2 
 #pragma unroll
         for (int q = 0; q < 16; q++) buf[pad16(base + q * Ns)] = make_float2(v[q].x, v[q].y);
       }
-      group_sync(T);
+      pass_sync<CTA_SYNC>(T);
     }
   }
 }

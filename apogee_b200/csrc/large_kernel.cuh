@@ -1,0 +1,203 @@
+// Fused matched filter for transforms larger than one CTA holds
+// (n = 32768 ... 1048576): a two-pass four-step through an L2-sized scratch.
+//
+// With n = N1 * N2, f = f1 + N1 f2 and k = N2 k1 + k2 (f1, k1 < N1; f2, k2 < N2):
+//
+//   z[N2 k1 + k2] = sum_f1 W_N1^(f1 k1) [ W_n^(f1 k2) sum_f2 P[f1 + N1 f2] W_N2^(f2 k2) ]
+//
+//   pass A  per (pair, column f1): conjugate product P = D conj(H) gathered along
+//           f2, N2-point inverse FFT, twiddle W_n^(f1 k2), store Y[k2][f1];
+//           16 adjacent columns per CTA so every load and store is coalesced.
+//   pass B  per (pair, row k2): N1-point inverse FFT of Y[k2][.], giving the lags
+//           N2 k1 + k2; per-bin argmax: shared-memory atomicMax inside the CTA on
+//           (|z|^2 bits << 32 | ~lag), then one 128-bit atomic compare-and-swap per
+//           (CTA, bin) that carries the winner's value with its key, so the
+//           correlation series is never written.
+//   finalize  candidate records -> (index, value) outputs and crossing counts.
+//
+// Pairs run in batches whose scratch (batch x n x 8 bytes, <= 64 MiB) stays
+// resident in the 126 MB L2; pairs are ordered template-major so the data rows
+// of one template share its spectrum in L2.  This is the unshipped "Tier C"
+// two-dispatch four-step of the reference (src/gpu/tierb.slang:1043-1150) and
+// the CPU plan of src/balanced-inl.h:174-386 for n up to 2^20, fused with the
+// product and the argmax as the single-CTA kernel is.
+#pragma once
+#include "flat_kernel.cuh"
+
+namespace mfb {
+
+constexpr int LARGE_MAX_BINS = 4096;
+constexpr int LARGE_COLS = 16;          // columns per pass-A CTA
+
+struct LargeArgs {
+  const float2 *data, *tmpl;            // rows of n complex64
+  int n, N1, N2;
+  int d0, nd, t0, nt;                   // pair block; output row = (d-d0)*nt + (t-t0)
+  const int32_t *list;                  // listed output rows, or nullptr (dense block)
+  long long total;                      // pairs in the dense block or the list
+  long long pair0;                      // first pair of this batch
+  int batch;                            // pairs in this batch
+  float2 *Y;                            // scratch [batch][N2][N1]
+  uint4 *rec;                           // [batch][nb] records {re, im, ~lag, |z|^2 bits}
+  const float2 *tw1, *tw2;              // inverse-pass twiddles of the N1- and N2-point FFTs
+  const float2 *tw_hi, *tw_lo;          // W_n^m = tw_hi[m >> lo_bits] * tw_lo[m & lo_mask]
+  int lo_bits;
+  int ws, we, binsize, nb;
+  float t2;
+  long long *out_idx;
+  float2 *out_val;
+  int rs;
+  int32_t *out_cnt;
+};
+
+// Output row and (d, t) of the pair with index pi (dense: template-major).
+__device__ __forceinline__ void large_pair(const LargeArgs &a, long long pi, int &row, int &d,
+                                           int &t) {
+  if (a.list) {
+    row = a.list[pi];
+    d = row / a.nt;
+    t = row - d * a.nt;
+  } else {
+    t = (int)(pi / a.nd);
+    d = (int)(pi - (long long)t * a.nd);
+    row = d * a.nt + t;
+  }
+}
+
+template <int N2>
+__global__ void __launch_bounds__(N2 >= 256 ? N2 : 256)
+large_pass_a(const LargeArgs a) {
+  constexpr int T2 = N2 / 16, C = LARGE_COLS;
+  static_assert(T2 * C == N2, "pass A runs one thread per (column, point group)");
+  extern __shared__ __align__(16) float2 smem[];
+  const int c = threadIdx.x % C, t = threadIdx.x / C;
+  float2 *buf = smem + c * FlatGeo<N2>::BUF;
+  const int tiles = a.N1 / C;
+  const long long work = (long long)a.batch * tiles;
+  const unsigned lo_mask = (1u << a.lo_bits) - 1u;
+  for (long long w = blockIdx.x; w < work; w += gridDim.x) {
+    const int bp = (int)(w / tiles), tile = (int)(w - (long long)bp * tiles);
+    const long long pi = a.pair0 + bp;
+    const int f1 = tile * C + c;
+    cf v[16];
+    if (pi < a.total) {
+      int row, d, tt;
+      large_pair(a, pi, row, d, tt);
+      const float2 *dp = a.data + (long long)(a.d0 + d) * a.n;
+      const float2 *hp = a.tmpl + (long long)(a.t0 + tt) * a.n;
+#pragma unroll
+      for (int s = 0; s < 16; s++) {
+        const long long f = f1 + (long long)a.N1 * (t + T2 * s);
+        const float2 x = __ldg(dp + f), h = __ldg(hp + f);
+        v[s].x = fmaf(x.x, h.x, x.y * h.y);
+        v[s].y = fmaf(x.y, h.x, -x.x * h.y);
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < 16; s++) v[s] = {0.f, 0.f};
+    }
+    inverse_passes<N2, true>(v, buf, a.tw2, t);
+    float2 *yp = a.Y + (long long)bp * a.N2 * a.N1 + f1;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int k2 = t + T2 * q;
+      const unsigned m = ((unsigned)f1 * (unsigned)k2) & (unsigned)(a.n - 1);
+      const float2 wh = __ldg(a.tw_hi + (m >> a.lo_bits)), wl = __ldg(a.tw_lo + (m & lo_mask));
+      const cf tw = cmul(cf{wh.x, wh.y}, cf{wl.x, wl.y});
+      const cf y = cmul(v[q], tw);
+      yp[(long long)k2 * a.N1] = make_float2(y.x, y.y);
+    }
+  }
+}
+
+// 128-bit max on the high 64 bits (the key); the low 64 bits (value) travel with it.
+__device__ __forceinline__ void rec_max(uint4 *slot, uint4 mine) {
+  unsigned __int128 *p = reinterpret_cast<unsigned __int128 *>(slot);
+  const unsigned __int128 m = ((unsigned __int128)(((unsigned long long)mine.w << 32) | mine.z) << 64) |
+                              (((unsigned long long)mine.y << 32) | mine.x);
+  const unsigned long long mkey = (unsigned long long)(m >> 64);
+  unsigned __int128 old = atomicCAS(p, (unsigned __int128)0, (unsigned __int128)0);  // atomic read
+  while ((unsigned long long)(old >> 64) < mkey) {
+    const unsigned __int128 prev = atomicCAS(p, old, m);
+    if (prev == old) break;
+    old = prev;
+  }
+}
+
+template <int N1>
+__global__ void __launch_bounds__(FlatGeo<N1>::CTA)
+large_pass_b(const LargeArgs a) {
+  using Geo = FlatGeo<N1>;
+  constexpr int T1 = Geo::T, G = Geo::G;
+  extern __shared__ __align__(16) float2 smem[];
+  const int g = threadIdx.x / T1, t = threadIdx.x % T1;
+  float2 *buf = smem + g * Geo::BUF;
+  unsigned long long *keys = reinterpret_cast<unsigned long long *>(smem + G * Geo::BUF);
+  const int bs = a.binsize;
+  const float inv_bs = 1.0f / (float)bs;
+  const long long work = (long long)a.batch * a.N2 / G;
+  for (long long w = blockIdx.x; w < work; w += gridDim.x) {
+    const long long r0 = w * G;                       // first row of this CTA
+    const int bp = (int)(r0 / a.N2), k2base = (int)(r0 - (long long)bp * a.N2);
+    const int k2 = k2base + g;
+    const bool live = a.pair0 + bp < a.total;
+    cf v[16];
+    const float2 *yp = a.Y + ((long long)bp * a.N2 + k2) * a.N1;
+#pragma unroll
+    for (int s = 0; s < 16; s++) {
+      const float2 x = yp[t + T1 * s];
+      v[s] = {x.x, x.y};
+    }
+    for (int b = threadIdx.x; b < a.nb; b += blockDim.x) keys[b] = 0ull;
+    __syncthreads();
+    inverse_passes<N1>(v, buf, a.tw1, t);
+    // thread t holds z[N2 k1 + k2] for k1 = t + T1 q
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int k1 = t + T1 * q;
+      const int lag = a.N2 * k1 + k2;
+      const float m2 = fmaf(v[q].x, v[q].x, v[q].y * v[q].y);
+      if (live && lag >= a.ws && lag < a.we && m2 > a.t2) {
+        const int bin = bin_of(lag - a.ws, bs, inv_bs);
+        atomicMax(keys + bin, ((unsigned long long)__float_as_uint(m2) << 32) | (unsigned)(~lag));
+        buf[pad16(k1)] = make_float2(v[q].x, v[q].y);
+      }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
+      const unsigned long long kk = keys[b];
+      if (kk == 0ull) continue;
+      const int lag = (int)(~(unsigned)kk);
+      const int gw = (lag % a.N2) - k2base, k1w = lag / a.N2;
+      const float2 val = smem[gw * Geo::BUF + pad16(k1w)];
+      rec_max(a.rec + (long long)bp * a.nb + b,
+              make_uint4(__float_as_uint(val.x), __float_as_uint(val.y), (unsigned)kk,
+                         (unsigned)(kk >> 32)));
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void large_finalize(const LargeArgs a) {
+  const long long n_out = (long long)a.batch * a.nb;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_out;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int bp = (int)(i / a.nb), b = (int)(i - (long long)bp * a.nb);
+    const long long pi = a.pair0 + bp;
+    if (pi >= a.total) continue;
+    int row, d, t;
+    large_pair(a, pi, row, d, t);
+    const uint4 r = a.rec[i];
+    const long long o = ((long long)row * a.nb + b) * a.rs;
+    if (r.w == 0u && r.z == 0u) {
+      a.out_idx[o] = -1;
+      a.out_val[o] = make_float2(0.f, 0.f);
+    } else {
+      a.out_idx[o] = (long long)(int)(~r.z);
+      a.out_val[o] = make_float2(__uint_as_float(r.x), __uint_as_float(r.y));
+      if (a.out_cnt) atomicAdd(a.out_cnt + row, 1);
+    }
+  }
+}
+
+}  // namespace mfb

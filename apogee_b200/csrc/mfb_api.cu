@@ -19,6 +19,7 @@
 #include "flat_kernel.cuh"
 #include "series_kernel.cuh"
 #include "hier_kernels.cuh"
+#include "large_kernel.cuh"
 
 using namespace mfb;
 
@@ -175,7 +176,108 @@ static cudaError_t launch_forward(int n, const NConst &c, const SeriesArgs &a, c
 }
 
 extern "C" int mfb_supported(size_t n) {
-  return n >= 64 && n <= 16384 && (n & (n - 1)) == 0;
+  return n >= 64 && n <= (1u << 20) && (n & (n - 1)) == 0;
+}
+
+static bool is_large(size_t n) { return n > 16384; }
+
+// ------------------------------------------------------------ large-n setup
+// n = N1 * N2 with N2 = 2^ceil(log2(n)/2) (<= 1024, the pass-A CTA size).
+struct LargeConst {
+  int N1 = 0, N2 = 0, lo_bits = 0;
+  float2 *tw_hi = nullptr, *tw_lo = nullptr;
+  NConst *c1 = nullptr, *c2 = nullptr;
+  int grid_a = 0, grid_b = 0, smem_a = 0, smem_b = 0, cta_a = 0, cta_b = 0;
+};
+static std::map<std::pair<int, int>, LargeConst> g_large;
+
+template <int N2>
+static int large_a_attr(int *grid, int *smem, int *cta, int sms) {
+  *smem = LARGE_COLS * FlatGeo<N2>::BUF * 8;
+  *cta = N2;
+  CUDA_TRY(cudaFuncSetAttribute(large_pass_a<N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
+  int b = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, large_pass_a<N2>, *cta, *smem));
+  if (b < 1) return fail(MFB_ERR_CUDA, "large pass A (N2=%d) cannot be resident", N2);
+  *grid = b * sms;
+  return MFB_OK;
+}
+template <int N1>
+static int large_b_attr(int *grid, int *smem, int *cta, int sms) {
+  *smem = FlatGeo<N1>::G * FlatGeo<N1>::BUF * 8 + LARGE_MAX_BINS * 8;
+  *cta = FlatGeo<N1>::CTA;
+  CUDA_TRY(cudaFuncSetAttribute(large_pass_b<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
+  int b = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, large_pass_b<N1>, *cta, *smem));
+  if (b < 1) return fail(MFB_ERR_CUDA, "large pass B (N1=%d) cannot be resident", N1);
+  *grid = b * sms;
+  return MFB_OK;
+}
+
+static int get_large(int device, int n, LargeConst **out) {
+  {
+    std::lock_guard<std::mutex> lk(g_const_mu);
+    auto it = g_large.find({device, n});
+    if (it != g_large.end()) { *out = &it->second; return MFB_OK; }
+  }
+  int L = 0;
+  while ((1 << L) < n) L++;
+  LargeConst c;
+  c.N2 = 1 << ((L + 1) / 2);
+  c.N1 = n / c.N2;
+  c.lo_bits = (L + 1) / 2;
+  int r = get_const(device, c.N1, &c.c1);
+  if (r == MFB_OK) r = get_const(device, c.N2, &c.c2);
+  if (r) return r;
+  std::vector<float2> hi((size_t)n >> c.lo_bits), lo((size_t)1 << c.lo_bits);
+  for (size_t i = 0; i < hi.size(); i++) hi[i] = unit_root((long long)(i << c.lo_bits), n);
+  for (size_t i = 0; i < lo.size(); i++) lo[i] = unit_root((long long)i, n);
+  CUDA_TRY(cudaMalloc(&c.tw_hi, hi.size() * sizeof(float2)));
+  CUDA_TRY(cudaMalloc(&c.tw_lo, lo.size() * sizeof(float2)));
+  CUDA_TRY(cudaMemcpy(c.tw_hi, hi.data(), hi.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(c.tw_lo, lo.data(), lo.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  switch (c.N2) {
+    case 256: r = large_a_attr<256>(&c.grid_a, &c.smem_a, &c.cta_a, sms); break;
+    case 512: r = large_a_attr<512>(&c.grid_a, &c.smem_a, &c.cta_a, sms); break;
+    case 1024: r = large_a_attr<1024>(&c.grid_a, &c.smem_a, &c.cta_a, sms); break;
+    default: return fail(MFB_ERR_UNSUPPORTED, "no four-step split for n=%d", n);
+  }
+  if (r) return r;
+  switch (c.N1) {
+    case 128: r = large_b_attr<128>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
+    case 256: r = large_b_attr<256>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
+    case 512: r = large_b_attr<512>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
+    case 1024: r = large_b_attr<1024>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
+    default: return fail(MFB_ERR_UNSUPPORTED, "no four-step split for n=%d", n);
+  }
+  if (r) return r;
+  std::lock_guard<std::mutex> lk(g_const_mu);
+  *out = &(g_large[{device, n}] = c);
+  return MFB_OK;
+}
+
+static cudaError_t launch_large(const LargeConst &c, const LargeArgs &a, cudaStream_t s) {
+  switch (c.N2) {
+    case 256: large_pass_a<256><<<c.grid_a, c.cta_a, c.smem_a, s>>>(a); break;
+    case 512: large_pass_a<512><<<c.grid_a, c.cta_a, c.smem_a, s>>>(a); break;
+    default: large_pass_a<1024><<<c.grid_a, c.cta_a, c.smem_a, s>>>(a); break;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  switch (c.N1) {
+    case 128: large_pass_b<128><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a); break;
+    case 256: large_pass_b<256><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a); break;
+    case 512: large_pass_b<512><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a); break;
+    default: large_pass_b<1024><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a); break;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const long long outs = (long long)a.batch * a.nb;
+  const int blocks = (int)std::min<long long>((outs + 255) / 256, 4096);
+  large_finalize<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
 }
 
 extern "C" size_t mfb_nbins(size_t n, size_t binsize, size_t start, size_t end) {
@@ -199,6 +301,11 @@ struct mfb_plan {
   int starts_cap = 0;
   float2 *sspec = nullptr;
   int sspec_rows = 0;
+  // large-n (two-pass) state: constants, L2-sized scratch, candidate records
+  LargeConst *lc = nullptr;
+  float2 *lY = nullptr;
+  uint4 *lrec = nullptr;
+  int lbatch = 0;
 };
 
 struct DeviceGuard {
@@ -226,7 +333,7 @@ extern "C" int mfb_create(mfb_plan **out, size_t n, int ndata, int ntmpl, int de
   p->n = n;
   p->nd = ndata;
   p->nt = ntmpl;
-  int r = get_const(device, (int)n, &p->c);
+  int r = is_large(n) ? get_large(device, (int)n, &p->lc) : get_const(device, (int)n, &p->c);
   if (r != MFB_OK) { delete p; return r; }
   cudaError_t e1 = cudaMalloc(&p->data, (size_t)ndata * n * sizeof(float2));
   cudaError_t e2 = e1 == cudaSuccess ? cudaMalloc(&p->tmpl, (size_t)ntmpl * n * sizeof(float2)) : e1;
@@ -252,6 +359,8 @@ extern "C" int mfb_destroy(mfb_plan *p) {
   cudaFree(p->tmpl);
   cudaFree(p->starts_dev);
   cudaFree(p->sspec);
+  cudaFree(p->lY);
+  cudaFree(p->lrec);
   delete p;
   return MFB_OK;
 }
@@ -304,7 +413,7 @@ static FlatArgs base_args(const mfb_plan *p, int d0, int nd, int t0, int nt, siz
   a.tmpl = p->tmpl;
   a.data_stride = (long long)p->n;
   a.tmpl_stride = (long long)p->n;
-  a.twid = p->c->twid;
+  a.twid = p->c ? p->c->twid : nullptr;
   a.d0 = d0; a.nd = nd; a.t0 = t0; a.nt = nt;
   if (end > p->n) end = p->n;
   a.ws = (int)start;
@@ -313,6 +422,54 @@ static FlatArgs base_args(const mfb_plan *p, int d0, int nd, int t0, int nt, siz
   a.nb = (int)nb;
   a.t2 = threshold > 0.f ? threshold * threshold : 0.f;
   return a;
+}
+
+// Two-pass path for n > 16384.  list/nlist: listed output rows (host count),
+// or nullptr for the dense block.  Scratch is allocated on first use.
+static int run_large(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *list,
+                     long long nlist, size_t binsize, float threshold, size_t start, size_t end,
+                     size_t nb, int64_t *idx, void *val, int32_t *counts, int rs) {
+  if (nb > (size_t)LARGE_MAX_BINS)
+    return fail(MFB_ERR_UNSUPPORTED, "n=%zu supports at most %d bins per pair", p->n, LARGE_MAX_BINS);
+  const LargeConst &c = *p->lc;
+  if (!p->lY) {
+    const size_t per = p->n * sizeof(float2);
+    int b = (int)std::max<size_t>(1, ((size_t)64 << 20) / per);
+    CUDA_TRY(cudaMalloc(&p->lY, (size_t)b * per));
+    CUDA_TRY(cudaMalloc(&p->lrec, (size_t)b * LARGE_MAX_BINS * sizeof(uint4)));
+    p->lbatch = b;
+  }
+  if (end > p->n) end = p->n;
+  LargeArgs a;
+  memset(&a, 0, sizeof a);
+  a.data = p->data;
+  a.tmpl = p->tmpl;
+  a.n = (int)p->n; a.N1 = c.N1; a.N2 = c.N2;
+  a.d0 = d0; a.nd = nd; a.t0 = t0; a.nt = nt;
+  a.list = list;
+  a.total = list ? nlist : (long long)nd * nt;
+  a.Y = p->lY;
+  a.rec = p->lrec;
+  a.tw1 = c.c1->twid;
+  a.tw2 = c.c2->twid;
+  a.tw_hi = c.tw_hi;
+  a.tw_lo = c.tw_lo;
+  a.lo_bits = c.lo_bits;
+  a.ws = (int)start; a.we = (int)end;
+  a.binsize = binsize > p->n ? (int)p->n : (int)binsize;
+  a.nb = (int)nb;
+  a.t2 = threshold > 0.f ? threshold * threshold : 0.f;
+  a.out_idx = (long long *)idx;
+  a.out_val = (float2 *)val;
+  a.rs = rs;
+  a.out_cnt = counts;
+  for (long long p0 = 0; p0 < a.total; p0 += p->lbatch) {
+    a.pair0 = p0;
+    a.batch = (int)std::min<long long>(p->lbatch, a.total - p0);
+    CUDA_TRY(cudaMemsetAsync(p->lrec, 0, (size_t)a.batch * nb * sizeof(uint4), p->stream));
+    CUDA_TRY(launch_large(c, a, p->stream));
+  }
+  return MFB_OK;
 }
 
 static int run_impl(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
@@ -331,6 +488,9 @@ static int run_impl(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
   a.rs = rs;
   a.out_cnt = counts;
   if (counts) CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nd * nt * sizeof(int32_t), p->stream));
+  if (is_large(p->n))
+    return run_large(p, d0, nd, t0, nt, nullptr, 0, binsize, threshold, start, end, nb, idx, val,
+                     counts, rs);
   CUDA_TRY(launch_flat<MODE_PEAKS>((int)p->n, *p->c, a, p->stream));
   return MFB_OK;
 }
@@ -367,6 +527,15 @@ static int run_rows_impl(mfb_plan *p, int d0, int nd, int t0, int nt, const int3
   a.out_val = (float2 *)val;
   a.rs = rs;
   a.out_cnt = counts;   // rows not listed keep whatever the caller put there
+  if (is_large(p->n)) {
+    // the two-pass path sizes its batches on the host: read the row count
+    int32_t cnt = 0;
+    CUDA_TRY(cudaMemcpyAsync(&cnt, nrows, sizeof cnt, cudaMemcpyDeviceToHost, p->stream));
+    CUDA_TRY(cudaStreamSynchronize(p->stream));
+    if (cnt > max_rows) return fail(MFB_ERR_ARG, "row count %d exceeds max_rows %d", cnt, max_rows);
+    return run_large(p, d0, nd, t0, nt, rows, cnt, binsize, threshold, start, end, nb, idx, val,
+                     counts, rs);
+  }
   CUDA_TRY(launch_flat<MODE_PEAKS>((int)p->n, *p->c, a, p->stream));
   return MFB_OK;
 }
@@ -381,6 +550,8 @@ extern "C" int mfb_run_rows(mfb_plan *p, int d0, int nd, int t0, int nt, const i
 extern "C" int mfb_forward(mfb_plan *p, const void *series, size_t nseries,
                            const uint64_t *starts_dev, int nblocks, void *spectra) {
   if (!p) return fail(MFB_ERR_ARG, "null plan");
+  if (is_large(p->n))
+    return fail(MFB_ERR_UNSUPPORTED, "block forward transforms are built for n <= 16384");
   if (!series || !starts_dev || !spectra || nblocks < 1)
     return fail(MFB_ERR_ARG, "invalid forward-transform arguments");
   DeviceGuard dg(p->device);

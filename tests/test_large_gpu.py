@@ -1,0 +1,92 @@
+"""Transforms larger than one CTA (n = 32768 ... 2^20): the two-pass four-step
+path, against the FP64 oracle."""
+import numpy as np
+import pytest
+
+from oracle import oracle, parity
+
+pytestmark = pytest.mark.gpu
+
+
+def _mf():
+    import apogee_b200 as mf
+    return mf
+
+
+def noise(rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+@pytest.mark.parametrize("n", [32768, 65536, 131072, 262144])
+def test_large_parity(n):
+    mf = _mf()
+    rng = np.random.default_rng(n + 1)
+    nd, nt = 2, 3
+    D, H = noise(rng, (nd, n)), noise(rng, (nt, n))
+    f = mf.MatchedFilter(n, nd, nt)
+    f.set_data(D)
+    f.set_templates(H)
+    z = oracle.correlate(D, H)
+    for binsize, thr, win in [(n // 16, 0.0, None), (n // 64, 0.0, None), (4096, 0.0, None),
+                              (n // 100 + 7, 0.0, (13, n - 5)),
+                              (n // 8, 4.0 * np.sqrt(n), (n // 3, n)), (n, 0.0, None)]:
+        out, cnt = f.run(binsize=binsize, threshold=thr, window=win, counts=True)
+        bad = parity.compare(out["index"], out["value"], z, binsize, thr, win)
+        assert not bad, (binsize, thr, win, bad[:3])
+        np.testing.assert_array_equal(cnt, (out["index"] >= 0).sum(-1))
+
+
+def test_largest_length():
+    mf = _mf()
+    n = 1 << 20
+    rng = np.random.default_rng(3)
+    D, H = noise(rng, (1, n)), noise(rng, (2, n))
+    f = mf.MatchedFilter(n, 1, 2)
+    f.set_data(D)
+    f.set_templates(H)
+    out = f.run(binsize=n // 256)
+    assert not parity.compare(out["index"], out["value"], oracle.correlate(D, H), n // 256)
+
+
+def test_large_known_lag_and_subrange():
+    mf = _mf()
+    n = 262144
+    rng = np.random.default_rng(4)
+    x = noise(rng, n)
+    lags = (0, 1, 12345, n - 1)
+    H = np.stack([x * np.exp(2j * np.pi * np.arange(n) * lag / n) for lag in lags]).astype(np.complex64)
+    f = mf.MatchedFilter(n, 1, len(lags))
+    f.set_data(x[None])
+    f.set_templates(H)
+    out = f.run(binsize=n)
+    np.testing.assert_array_equal(out["index"][0, :, 0], lags)
+    sub = f.run(binsize=n, templates=(1, 2))
+    np.testing.assert_array_equal(sub["index"][0, :, 0], lags[1:3])
+
+
+def test_large_too_many_bins_refused():
+    mf = _mf()
+    n = 65536
+    f = mf.MatchedFilter(n, 1, 1)
+    f.set_data(np.ones((1, n), np.complex64))
+    f.set_templates(np.ones((1, n), np.complex64))
+    with pytest.raises(ValueError):
+        f.run(binsize=8)
+
+
+def test_large_hierarchical_refine_is_flat():
+    """Gate 0 refines every pair: the hierarchical result equals the flat one."""
+    mf = _mf()
+    n, nd, nt = 65536, 2, 3
+    rng = np.random.default_rng(5)
+    D, H = noise(rng, (nd, n)), noise(rng, (nt, n))
+    flat = mf.MatchedFilter(n, nd, nt)
+    hf = mf.HierarchicalFilter(n, nd, nt, band=n // 16, coarse="fp32")
+    hf.set_coarse_threshold(0.0)
+    for o in (flat, hf):
+        o.set_data(D)
+        o.set_templates(H)
+    a = flat.run(binsize=n // 16).copy()
+    b = hf.run(binsize=n // 16)
+    np.testing.assert_array_equal(a, b)
+    assert hf.stats == (nd * nt, nd * nt)
