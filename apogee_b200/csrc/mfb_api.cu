@@ -1014,3 +1014,180 @@ extern "C" int mfb_fp32_peak(int device, double *flops_per_s) {
   *flops_per_s = 2.0 * fmas / (ms * 1e-3);
   return MFB_OK;
 }
+
+// ------------------------------------------ large transforms without allocation
+// Some callers cannot let a library allocate device memory: a serving process
+// that hands all of HBM to its own pool or arena at start-up leaves nothing for
+// cudaMalloc, and a pipeline on a latency budget cannot absorb the device-wide
+// synchronisation that cudaMalloc and cudaFree imply while its other streams
+// run.  mfb_run_large_static serves them with the two-pass filter for large n:
+// no plan, device inputs and outputs from the caller, and its scratch (the
+// pass-A rows and the per-bin records) in the file-scope array below, reserved
+// with the module.  Its twiddles sit in a second file-scope table, uploaded
+// once per device by the set-up of the first call on that device.
+constexpr int STATIC_MIN_LOG = 15, STATIC_MAX_LOG = 19;   // n = 32768 ... 524288
+constexpr int kStaticFft[4] = {128, 256, 512, 1024};      // N1 and N2 of those n
+
+constexpr int static_fft_count(int N) {
+  return N == 128 ? twiddle_count<128>()
+       : N == 256 ? twiddle_count<256>()
+       : N == 512 ? twiddle_count<512>()
+                  : twiddle_count<1024>();
+}
+// Offset of the inter-pass table of the N-point FFT.
+constexpr int static_fft_off(int N) {
+  int o = 0;
+  for (int i = 0; i < 4 && kStaticFft[i] < N; i++) o += static_fft_count(kStaticFft[i]);
+  return o;
+}
+// Offset of the W_n hi table of n = 2^L (its lo table follows it).
+constexpr int static_root_off(int L) {
+  int o = static_fft_off(2048);
+  for (int l = STATIC_MIN_LOG; l < L; l++) o += (1 << (l - (l + 1) / 2)) + (1 << ((l + 1) / 2));
+  return o;
+}
+constexpr int STATIC_TW_COUNT = static_root_off(STATIC_MAX_LOG + 1);
+
+static __device__ __align__(256) unsigned char g_static_scratch[MFB_STATIC_SCRATCH_BYTES];
+static __device__ __align__(256) float2 g_static_twiddles[STATIC_TW_COUNT];
+
+struct StaticDev {
+  bool ready = false;
+  unsigned char *scratch = nullptr;     // device address of g_static_scratch
+  float2 *tw = nullptr;                 // device address of g_static_twiddles
+  LargeConst shape[STATIC_MAX_LOG + 1]; // launch shapes per log2(n)
+};
+constexpr int STATIC_MAX_DEVICES = 64;
+static std::mutex g_static_mu;
+static StaticDev g_static[STATIC_MAX_DEVICES];
+
+// Once per device, with that device current: the symbol addresses, the twiddle
+// upload and the kernel attributes.  Synchronous, so it must not run inside a
+// stream capture.
+static int static_setup(int device, StaticDev **out) {
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  StaticDev &s = g_static[device];
+  if (!s.ready) {
+    void *ptr = nullptr;
+    CUDA_TRY(cudaGetSymbolAddress(&ptr, g_static_scratch));
+    s.scratch = (unsigned char *)ptr;
+    CUDA_TRY(cudaGetSymbolAddress(&ptr, g_static_twiddles));
+    s.tw = (float2 *)ptr;
+    std::vector<float2> tw(STATIC_TW_COUNT);
+    auto put = [&](int N, const std::vector<float2> &t) {
+      std::copy(t.begin(), t.begin() + static_fft_count(N), tw.begin() + static_fft_off(N));
+    };
+    put(128, build_twiddles<128>());
+    put(256, build_twiddles<256>());
+    put(512, build_twiddles<512>());
+    put(1024, build_twiddles<1024>());
+    for (int L = STATIC_MIN_LOG; L <= STATIC_MAX_LOG; L++) {
+      const int lo_bits = (L + 1) / 2, n = 1 << L;
+      float2 *hi = tw.data() + static_root_off(L), *lo = hi + (n >> lo_bits);
+      for (int i = 0; i < (n >> lo_bits); i++) hi[i] = unit_root((long long)i << lo_bits, n);
+      for (int i = 0; i < (1 << lo_bits); i++) lo[i] = unit_root(i, n);
+    }
+    CUDA_TRY(cudaMemcpy(s.tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    int sms = 0, r = MFB_OK;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    for (int L = STATIC_MIN_LOG; L <= STATIC_MAX_LOG && r == MFB_OK; L++) {
+      LargeConst &c = s.shape[L];
+      c.lo_bits = (L + 1) / 2;
+      c.N2 = 1 << c.lo_bits;
+      c.N1 = 1 << (L - c.lo_bits);
+      switch (c.N2) {
+        case 256: r = large_a_attr<256>(&c.grid_a, &c.smem_a, &c.cta_a, sms); break;
+        case 512: r = large_a_attr<512>(&c.grid_a, &c.smem_a, &c.cta_a, sms); break;
+        default: r = large_a_attr<1024>(&c.grid_a, &c.smem_a, &c.cta_a, sms); break;
+      }
+      if (r) break;
+      switch (c.N1) {
+        case 128: r = large_b_attr<128>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
+        case 256: r = large_b_attr<256>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
+        default: r = large_b_attr<512>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
+      }
+    }
+    if (r) return r;
+    s.ready = true;
+  }
+  *out = &s;
+  return MFB_OK;
+}
+
+extern "C" int mfb_run_large_static(int device, size_t n, const void *data, int nd,
+                                    const void *templates, int nt, size_t binsize,
+                                    float threshold, size_t start, size_t end, int64_t *idx,
+                                    void *val, int32_t *counts, void *stream) {
+  if (!data || !templates || !idx || !val) return fail(MFB_ERR_ARG, "null pointer");
+  if (nd < 1 || nt < 1) return fail(MFB_ERR_ARG, "ndata and ntemplates must be >= 1");
+  if (std::isnan(threshold)) return fail(MFB_ERR_ARG, "threshold is NaN");
+  int L = 0;
+  while (L < 62 && ((size_t)1 << L) < n) L++;
+  if (((size_t)1 << L) != n || L < STATIC_MIN_LOG)
+    return fail(MFB_ERR_UNSUPPORTED,
+                "mfb_run_large_static: n=%zu is not a power of two >= 32768 (mfb_run covers it)", n);
+  const size_t nb = mfb_nbins(n, binsize, start, end);
+  if (nb == 0) return fail(MFB_ERR_ARG, "zero binsize or empty window [%zu, %zu)", start, end);
+  if (nb > (size_t)LARGE_MAX_BINS)
+    return fail(MFB_ERR_UNSUPPORTED, "mfb_run_large_static: %zu bins per pair; at most %d",
+                nb, LARGE_MAX_BINS);
+  const size_t rec_one = (nb * sizeof(uint4) + 255) & ~(size_t)255;
+  const size_t need = rec_one + n * sizeof(float2);
+  if (need > (size_t)MFB_STATIC_SCRATCH_BYTES || L > STATIC_MAX_LOG)
+    return fail(MFB_ERR_UNSUPPORTED,
+                "mfb_run_large_static: n=%zu needs %zu bytes of scratch for one pair; the static "
+                "scratch holds %zu (MFB_STATIC_SCRATCH_BYTES)",
+                n, need, (size_t)MFB_STATIC_SCRATCH_BYTES);
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev || device >= STATIC_MAX_DEVICES)
+    return fail(MFB_ERR_ARG, "no device %d", device);
+  DeviceGuard dg(device);
+  StaticDev *s = nullptr;
+  int r = static_setup(device, &s);
+  if (r) return r;
+  // Pairs per batch: records [batch][nb] first, then rows [batch][n].
+  long long batch = (long long)(MFB_STATIC_SCRATCH_BYTES / (nb * sizeof(uint4) + n * sizeof(float2)));
+  auto bytes = [&](long long b) {
+    return ((b * nb * sizeof(uint4) + 255) & ~(size_t)255) + b * n * sizeof(float2);
+  };
+  while (batch > 1 && bytes(batch) > (size_t)MFB_STATIC_SCRATCH_BYTES) batch--;
+  const long long total = (long long)nd * nt;
+  if (batch > total) batch = total;
+  const LargeConst &c = s->shape[L];
+  uint4 *rec = reinterpret_cast<uint4 *>(s->scratch);
+  float2 *Y = reinterpret_cast<float2 *>(s->scratch + ((batch * nb * sizeof(uint4) + 255) & ~(size_t)255));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (end > n) end = n;
+  LargeArgs a;
+  memset(&a, 0, sizeof a);
+  a.data = (const float2 *)data;
+  a.tmpl = (const float2 *)templates;
+  a.n = (int)n; a.N1 = c.N1; a.N2 = c.N2;
+  a.d0 = 0; a.nd = nd; a.t0 = 0; a.nt = nt;
+  a.list = nullptr;
+  a.total = total;
+  a.Y = Y;
+  a.rec = rec;
+  a.tw1 = s->tw + static_fft_off(c.N1);
+  a.tw2 = s->tw + static_fft_off(c.N2);
+  a.tw_hi = s->tw + static_root_off(L);
+  a.tw_lo = a.tw_hi + (n >> c.lo_bits);
+  a.lo_bits = c.lo_bits;
+  a.ws = (int)start; a.we = (int)end;
+  a.binsize = binsize > n ? (int)n : (int)binsize;
+  a.nb = (int)nb;
+  a.t2 = threshold > 0.f ? threshold * threshold : 0.f;
+  a.out_idx = (long long *)idx;
+  a.out_val = (float2 *)val;
+  a.rs = 1;
+  a.out_cnt = counts;
+  if (counts) CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)total * sizeof(int32_t), st));
+  for (long long p0 = 0; p0 < total; p0 += batch) {
+    a.pair0 = p0;
+    a.batch = (int)std::min<long long>(batch, total - p0);
+    CUDA_TRY(cudaMemsetAsync(rec, 0, (size_t)a.batch * nb * sizeof(uint4), st));
+    CUDA_TRY(launch_large(c, a, st));
+  }
+  return MFB_OK;
+}

@@ -152,6 +152,41 @@ int mfb_hier_config(mfb_hplan *p, size_t *band, int *coarse_kind);
 int mfb_hier_coarse_values(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t start,
                            size_t end, float *out);
 
+/* ---- large transforms with no allocation --------------------------------- */
+
+/* Size of the file-scope device array that mfb_run_large_static uses as its
+   scratch: 8 MiB per device, reserved when the library's device code loads. */
+#define MFB_STATIC_SCRATCH_BYTES (8u << 20)
+
+/* No counterpart in the reference.  The two-pass filter of mfb_run for
+   power-of-two n = 32768 ... 524288 with no plan and no allocation of any
+   kind, for callers that cannot let a library allocate device memory (their
+   own pool owns HBM, or the device-wide synchronisation of cudaMalloc/cudaFree
+   would stall their other streams).
+   data [nd][n], templates [nt][n]: complex64 rows in DEVICE memory of `device`.
+   idx int64 / val complex64 [nd][nt][nb] DEVICE outputs with
+   nb = mfb_nbins(n, binsize, start, end) <= 4096; counts int32 [nd*nt] or
+   NULL.  Results, threshold and window mean what they mean for mfb_run.  Work
+   is queued on `stream` (a cudaStream_t of `device`; NULL = default stream).
+   Limit: one pair needs n*8 bytes of rows plus nb*16 bytes of records
+   (rounded up to 256); that must fit MFB_STATIC_SCRATCH_BYTES, so n = 1048576
+   is refused with MFB_ERR_UNSUPPORTED and a message giving the bytes needed.
+   Pairs run in as many batches as the scratch needs.
+   Zeroing: the records must be zero when each batch's second pass starts;
+   the call clears them on `stream` itself, and clears counts, so nothing the
+   caller passes has to start at zero and nothing carries over between calls.
+   Set-up: the first call on a device takes the scratch's device address
+   (cudaGetSymbolAddress, with that device current), uploads the twiddles and
+   sets the kernel attributes, synchronously; make that first call before any
+   stream capture.
+   Races: the scratch is one per device, so calls on one device that overlap
+   in time (two streams without an ordering between them, or two host
+   threads) overwrite each other's scratch and return wrong results; order
+   them on one stream or with events. */
+int mfb_run_large_static(int device, size_t n, const void *data, int nd, const void *templates,
+                         int nt, size_t binsize, float threshold, size_t start, size_t end,
+                         int64_t *idx, void *val, int32_t *counts, void *stream);
+
 /* ---- measurement --------------------------------------------------------- */
 
 /* Measured FP32 FMA throughput of `device` in FLOP/s (2 per FMA), from a
