@@ -61,7 +61,8 @@ SIGNATURES = {
     "mfb_hier_config": (_I, [_P, _SZP, _IP]),
     "mfb_hier_coarse_values": (_I, [_P, _I, _I, _I, _I, _SZ, _SZ, _P]),
     "mfb_fp32_peak": (_I, [_I, _DP]),
-    "mfb_run_large_static": (_I, [_I, _SZ, _P, _I, _P, _I, _SZ, _F, _SZ, _SZ, _P, _P, _P, _P]),
+    "mfb_adjoint": (_I, [_I, _SZ, _P, _I, _P, _I, _SZ, _P, _P, _P, _P, _P]),
+    "mfb_run_large_static":(_I, [_I, _SZ, _P, _I, _P, _I, _SZ, _F, _SZ, _SZ, _P, _P, _P, _P]),
 }
 
 _LIB = None

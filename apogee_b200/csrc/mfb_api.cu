@@ -20,6 +20,7 @@
 #include "series_kernel.cuh"
 #include "hier_kernels.cuh"
 #include "large_kernel.cuh"
+#include "adjoint_kernel.cuh"
 
 using namespace mfb;
 
@@ -1188,6 +1189,112 @@ extern "C" int mfb_run_large_static(int device, size_t n, const void *data, int 
     a.batch = (int)std::min<long long>(batch, total - p0);
     CUDA_TRY(cudaMemsetAsync(rec, 0, (size_t)a.batch * nb * sizeof(uint4), st));
     CUDA_TRY(launch_large(c, a, st));
+  }
+  return MFB_OK;
+}
+
+// ---------------------------------------------------------------- adjoint
+// W_n^m twiddles for the adjoint kernel: hi[m >> lo_bits] * lo[m & mask],
+// built once per (device, n) from FP64 roots.
+struct AdjTables {
+  float2 *hi = nullptr, *lo = nullptr;
+  int lo_bits = 0, hi_count = 0;
+};
+static std::map<std::pair<int, int>, AdjTables> g_adj;
+
+static int get_adj_tables(int device, int n, AdjTables **out) {
+  std::lock_guard<std::mutex> lk(g_const_mu);
+  auto it = g_adj.find({device, n});
+  if (it != g_adj.end()) { *out = &it->second; return MFB_OK; }
+  int L = 0;
+  while ((1 << L) < n) L++;
+  AdjTables t;
+  t.lo_bits = (L + 1) / 2;
+  t.hi_count = n >> t.lo_bits;
+  std::vector<float2> hi(t.hi_count), lo((size_t)1 << t.lo_bits);
+  for (int i = 0; i < t.hi_count; i++) hi[i] = unit_root((long long)i << t.lo_bits, n);
+  for (size_t i = 0; i < lo.size(); i++) lo[i] = unit_root((long long)i, n);
+  CUDA_TRY(cudaMalloc(&t.hi, hi.size() * sizeof(float2)));
+  CUDA_TRY(cudaMalloc(&t.lo, lo.size() * sizeof(float2)));
+  CUDA_TRY(cudaMemcpy(t.hi, hi.data(), hi.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(t.lo, lo.data(), lo.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  *out = &(g_adj[{device, n}] = t);
+  return MFB_OK;
+}
+
+template <bool GD>
+static cudaError_t launch_adjoint(int oc, dim3 grid, const AdjArgs &a, cudaStream_t s) {
+  switch (oc) {
+    case 8: adjoint_kernel<8, GD><<<grid, ADJ_THREADS, 0, s>>>(a); break;
+    case 4: adjoint_kernel<4, GD><<<grid, ADJ_THREADS, 0, s>>>(a); break;
+    case 2: adjoint_kernel<2, GD><<<grid, ADJ_THREADS, 0, s>>>(a); break;
+    default: adjoint_kernel<1, GD><<<grid, ADJ_THREADS, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+// One side of the adjoint: own rows per CTA (OC) shrink, and then the summed
+// rows split over blockIdx.z with atomic accumulation, until the grid covers
+// the device about twice.
+static int adjoint_side(bool grad_data, int n, int nd, int nt, int nb, const float2 *src,
+                        const int64_t *idx, const float2 *gz, float2 *out, const AdjTables &tw,
+                        int sms, cudaStream_t st) {
+  AdjArgs a;
+  memset(&a, 0, sizeof a);
+  a.src = src; a.idx = idx; a.gz = gz; a.out = out;
+  a.n = n; a.nd = nd; a.nt = nt; a.nb = nb;
+  a.own = grad_data ? nd : nt;
+  a.other = grad_data ? nt : nd;
+  a.tw_hi = tw.hi; a.tw_lo = tw.lo; a.lo_bits = tw.lo_bits; a.hi_count = tw.hi_count;
+  const long long fx = ((n >> 1) + ADJ_THREADS - 1) / ADJ_THREADS;
+  const long long target = 2LL * sms;
+  int oc = 8;
+  while (oc > 1 && fx * ((a.own + oc - 1) / oc) < target) oc >>= 1;
+  const long long chunks = (a.own + oc - 1) / oc;
+  if (chunks > 65535) return fail(MFB_ERR_UNSUPPORTED, "adjoint: too many rows (%d)", a.own);
+  long long split = 1;
+  if (fx * chunks < target) split = std::min<long long>(a.other, (target + fx * chunks - 1) / (fx * chunks));
+  a.other_per_split = (int)((a.other + split - 1) / split);
+  split = (a.other + a.other_per_split - 1) / a.other_per_split;
+  if ((long long)oc * nb <= ADJ_CAP) {
+    a.bins_per_round = nb;
+    a.rows_per_round = ADJ_CAP / (oc * nb);
+  } else {
+    a.bins_per_round = ADJ_CAP / oc;
+    a.rows_per_round = 1;
+  }
+  a.accumulate = split > 1;
+  if (a.accumulate) CUDA_TRY(cudaMemsetAsync(out, 0, (size_t)a.own * n * sizeof(float2), st));
+  const dim3 grid((unsigned)fx, (unsigned)chunks, (unsigned)split);
+  CUDA_TRY(grad_data ? launch_adjoint<true>(oc, grid, a, st) : launch_adjoint<false>(oc, grid, a, st));
+  return MFB_OK;
+}
+
+extern "C" int mfb_adjoint(int device, size_t n, const void *data, int nd, const void *templates,
+                           int nt, size_t nb, const int64_t *idx, const void *gz, void *grad_data,
+                           void *grad_tmpl, void *stream) {
+  if (!mfb_supported(n)) return fail(MFB_ERR_UNSUPPORTED, "adjoint: unsupported n=%zu", n);
+  if (nd < 1 || nt < 1 || nb < 1 || nb > n) return fail(MFB_ERR_ARG, "adjoint: bad shape");
+  if (!data || !templates || !idx || !gz) return fail(MFB_ERR_ARG, "adjoint: null input");
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(MFB_ERR_ARG, "no device %d", device);
+  DeviceGuard dg(device);
+  AdjTables *tw = nullptr;
+  int r = get_adj_tables(device, (int)n, &tw);
+  if (r) return r;
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (grad_data) {
+    r = adjoint_side(true, (int)n, nd, nt, (int)nb, (const float2 *)templates, idx,
+                     (const float2 *)gz, (float2 *)grad_data, *tw, sms, st);
+    if (r) return r;
+  }
+  if (grad_tmpl) {
+    r = adjoint_side(false, (int)n, nd, nt, (int)nb, (const float2 *)data, idx,
+                     (const float2 *)gz, (float2 *)grad_tmpl, *tw, sms, st);
+    if (r) return r;
   }
   return MFB_OK;
 }

@@ -34,6 +34,28 @@ def template_bank(n, nt, rng, kmin=20, kmax=None):
     return H.astype(np.complex64)
 
 
+def template_bank_torch(n, alpha, tc, kmin=20, kmax=None):
+    """template_bank's formula in torch, differentiable in ``alpha`` and ``tc``
+    (1-D tensors of one value per template); float64 parameters give
+    complex128 templates [nt][n]."""
+    import torch
+    kmax = n // 2 - 1 if kmax is None else int(kmax)
+    k = torch.arange(kmin, kmax + 1, dtype=alpha.dtype, device=alpha.device)
+    phase = 2 * torch.pi * k * tc[:, None] / n + alpha[:, None] * k ** (-5.0 / 3.0)
+    amp = k ** (-7.0 / 6.0)
+    half = torch.polar(amp.expand_as(phase), phase)
+    nt = alpha.shape[0]
+
+    def zeros(width):
+        return torch.zeros(nt, width, dtype=half.dtype, device=half.device)
+
+    # bins: [0, kmin) zero | [kmin, kmax] half | (kmax, n-kmax) zero
+    #       | [n-kmax, n-kmin] conjugate mirror | (n-kmin, n) zero
+    mirror = torch.conj(torch.flip(half, dims=[1]))
+    H = torch.cat([zeros(kmin), half, zeros(n - 2 * kmax - 1), mirror, zeros(kmin - 1)], dim=1)
+    return H / torch.linalg.vector_norm(H, dim=1, keepdim=True)
+
+
 def noise_spectra(n, nd, rng):
     """FFT of real N(0,1) noise / sqrt(n), exactly Hermitian."""
     x = rng.standard_normal((nd, n))

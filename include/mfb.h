@@ -152,6 +152,23 @@ int mfb_hier_config(mfb_hplan *p, size_t *band, int *coarse_kind);
 int mfb_hier_coarse_values(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t start,
                            size_t end, float *out);
 
+/* ---- adjoint --------------------------------------------------------------- */
+
+/* No counterpart in the reference (it has no gradients).  Adjoint of the peak
+   values at their fixed lags: with k = idx[d][t][b] (skipped when < 0) and g =
+   gz[d][t][b] the upstream gradient of the complex peak value in torch's
+   convention (dL/dRe z + i dL/dIm z),
+     grad_data[d][f] = sum_t sum_b g       * templates[t][f] * exp(-2 pi i f k / n)
+     grad_tmpl[t][f] = sum_d sum_b conj(g) * data[d][f]      * exp(+2 pi i f k / n)
+   data [nd][n], templates [nt][n], gz, grad_*: complex64; idx int64
+   [nd][nt][nb]; all DEVICE pointers of `device`.  Either gradient may be NULL;
+   each given one is overwritten.  FP32 arithmetic with FP64-built twiddles.
+   Queued on `stream` (NULL = default); the first call for an n builds its
+   twiddle tables (allocates, synchronises). */
+int mfb_adjoint(int device, size_t n, const void *data, int nd, const void *templates, int nt,
+                size_t nb, const int64_t *idx, const void *gz, void *grad_data, void *grad_tmpl,
+                void *stream);
+
 /* ---- large transforms with no allocation --------------------------------- */
 
 /* Size of the file-scope device array that mfb_run_large_static uses as its
