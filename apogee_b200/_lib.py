@@ -32,7 +32,40 @@ _SZP = ctypes.POINTER(ctypes.c_size_t)
 _IP = ctypes.POINTER(ctypes.c_int)
 _DP = ctypes.POINTER(ctypes.c_double)
 
+
+
+class MfbJob(ctypes.Structure):
+    """struct mfb_job of include/mfb.h (field order and types as declared)."""
+    _fields_ = [
+        ("n", ctypes.c_size_t),
+        ("nd", ctypes.c_int),
+        ("nt", ctypes.c_int),
+        ("data", ctypes.c_void_p),
+        ("templates", ctypes.c_void_p),
+        ("series", ctypes.c_void_p),
+        ("nseries", ctypes.c_size_t),
+        ("starts", ctypes.c_void_p),
+        ("binsize", ctypes.c_size_t),
+        ("threshold", ctypes.c_float),
+        ("start", ctypes.c_size_t),
+        ("end", ctypes.c_size_t),
+        ("records", ctypes.c_void_p),
+        ("split", ctypes.c_int),
+        ("unit_items", ctypes.c_int),
+    ]
+
+
+class MfbBatchOpts(ctypes.Structure):
+    """struct mfb_batch_opts of include/mfb.h."""
+    _fields_ = [("slot_bytes", ctypes.c_size_t), ("slots", ctypes.c_int)]
+
+
 SIGNATURES = {
+    "mfb_batch_create": (_I, [_PP, _I, ctypes.POINTER(MfbJob), _I, ctypes.POINTER(MfbBatchOpts)]),
+    "mfb_batch_run": (_I, [_P, _P]),
+    "mfb_batch_status": (_I, [_P, _P]),
+    "mfb_batch_info": (_I, [_P, _I64P, _IP, _IP, _IP, _SZP]),
+    "mfb_batch_destroy": (_I, [_P]),
     "mfb_create": (_I, [_PP, _SZ, _I, _I, _I]),
     "mfb_destroy": (_I, [_P]),
     "mfb_set_stream": (_I, [_P, _P]),

@@ -1,0 +1,118 @@
+"""Autotuner for the batched launch.
+
+For one transform length n it times every candidate configuration of the
+batched kernel on the device, in a one-job batch with a probe workload of
+that n, and keeps the fastest:
+
+* n <= 4096 (single-CTA fused filter): pairs per ticket -- 1, 2, 4 or 8
+  items of 4096/n pairs (longer tickets take fewer queue atomics, shorter
+  ones balance the tail better);
+* n >= 8192 (four-step): the factorisation n = N1 * N2 with N2 in
+  {64, 128, 256} and 64 <= N1 <= 4096, i.e. which radix-16 transform sizes
+  the two passes run, and so the column tile width 4096/N2 of the first pass.
+
+Results are cached per (device name, n) for the process, and in a JSON file
+when ``MFB_TUNE_CACHE`` names one.
+"""
+import json
+import os
+
+_CACHE = {}
+
+
+def candidates(n):
+    """Configurations the batched kernel accepts for transform length n."""
+    if n <= 4096:
+        return [{"unit_items": k} for k in (1, 2, 4, 8)]
+    out = []
+    for n2 in (64, 128, 256):
+        if 64 <= n // n2 <= 4096:
+            out.append({"split": n2})
+    return out
+
+
+def default(n):
+    """The configuration the library uses without tuning."""
+    if n <= 4096:
+        return {"unit_items": 1}
+    return {"split": 256 if n >= 16384 else 128}
+
+
+def _load_file():
+    path = os.environ.get("MFB_TUNE_CACHE")
+    if not path or not os.path.exists(path):
+        return {}
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store_file(key, cfg):
+    path = os.environ.get("MFB_TUNE_CACHE")
+    if not path:
+        return
+    data = _load_file()
+    data[key] = cfg
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def probe_shape(n, points=1 << 25):
+    """(nd, nt) of the probe workload: about `points` correlation samples."""
+    nd = 8
+    nt = int(max(16, min(4096, points // (n * nd))))
+    return nd, nt
+
+
+def tune(n, device=None, reps=3, warmup=2):
+    """Fastest configuration for n on `device` (a Device, spec or None)."""
+    import torch
+    from .batch import BatchedFilter, Job
+    from .device import parse
+    dev = parse(device)
+    key = "%s|%d" % (dev.name or str(dev), n)
+    if key in _CACHE:
+        return dict(_CACHE[key])
+    stored = _load_file().get(key)
+    if stored is not None:
+        _CACHE[key] = stored
+        return dict(stored)
+    cands = candidates(n)
+    if len(cands) == 1:
+        _CACHE[key] = cands[0]
+        return dict(cands[0])
+    nd, nt = probe_shape(n)
+    tdev = torch.device("cuda", dev.index)
+    g = torch.Generator(device=tdev).manual_seed(n)
+    D = torch.randn(nd, n, dtype=torch.complex64, device=tdev, generator=g)
+    H = torch.randn(nt, n, dtype=torch.complex64, device=tdev, generator=g)
+    best, best_ms = None, float("inf")
+    for cfg in cands:
+        bf = BatchedFilter([Job(H, data=D, binsize=max(1, n // 16))], device=dev,
+                           tune={n: cfg})
+        for _ in range(warmup):
+            bf.run()
+        bf.wait()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            bf.run()
+        b.record()
+        bf.wait()
+        ms = a.elapsed_time(b) / reps
+        bf.close()
+        if ms < best_ms:
+            best, best_ms = cfg, ms
+    _CACHE[key] = best
+    _store_file(key, best)
+    return dict(best)
+
+
+def tuned():
+    """The configurations tuned so far in this process: {key: config}."""
+    return dict(_CACHE)

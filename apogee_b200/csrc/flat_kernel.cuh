@@ -59,6 +59,7 @@ struct FlatArgs {
   int32_t *fire_count;        // device counter (zeroed before the launch)
   int full_nb;                // bins of the full-size output written as (-1,0) when dismissed
   float *coarse_out;          // if set: write max |z| over the window per row instead of gating
+  int data_cg;                // 1: data rows were written in this launch (coherent loads)
 };
 
 template <int N>
@@ -203,25 +204,26 @@ __device__ __forceinline__ void inverse_passes(cf *v, float2 *buf, const float2 
   }
 }
 
-template <int N, int MODE>
-__global__ void __launch_bounds__(FlatGeo<N>::CTA, FlatGeo<N>::CTA <= 256 ? 2 : 1)
-flat_kernel(const FlatArgs a) {
+// Items [ibeg, iend) of one launch's pairs (item i = pairs i*G .. i*G+G-1 of
+// the dense block or the list), processed by one CTA of FlatGeo<N>::CTA
+// threads with `smem` its dynamic shared memory.  CACHE_D keeps a data row
+// in registers while consecutive pairs share it (long static ranges); without
+// it the data spectrum is loaded beside each template (short dynamic ranges,
+// 32 registers fewer).  Used by flat_kernel (a
+// static range per CTA) and by the batched kernel (ranges handed out at run
+// time); synchronises the CTA on entry, so smem may still be in use then.
+template <int N, int MODE, bool CACHE_D = true>
+__device__ __forceinline__ void flat_range(const FlatArgs &a, long long ibeg, long long iend,
+                                           float2 *smem) {
   using Geo = FlatGeo<N>;
   constexpr int T = Geo::T, G = Geo::G;
-  extern __shared__ __align__(16) float2 smem[];
-
   const int g = threadIdx.x / T;          // pair slot inside the CTA
   const int t = threadIdx.x % T;          // thread inside the pair
   float2 *buf = smem + g * Geo::BUF;
-
-  // Work: dense block or a device list of output rows.
   const long long total = a.list ? (long long)(*a.list_count) : (long long)a.nd * a.nt;
-  const long long items = (total + G - 1) / G;
-  const long long per = items / gridDim.x, extra = items % gridDim.x;
-  const long long ibeg = blockIdx.x * per + (blockIdx.x < extra ? blockIdx.x : extra);
-  const long long iend = ibeg + per + (blockIdx.x < extra ? 1 : 0);
+  __syncthreads();
 
-  cf dreg[16];
+  cf dreg[CACHE_D ? 16 : 1];   // the data row, kept while consecutive pairs share it
   int cur_d = -1;
   const int lane = threadIdx.x & 31;
 
@@ -275,22 +277,40 @@ flat_kernel(const FlatArgs a) {
     // ---- pass 0: load, conjugate product, radix-R0 butterflies ----------
     cf v[16];
     if (live) {
-      if (d != cur_d) {
-        const float2 *dp = a.data + (long long)(a.d0 + d) * a.data_stride;
+      const float2 *hp = a.tmpl + (long long)(a.t0 + tt) * a.tmpl_stride;
+      const float2 *dp = a.data + (long long)(a.d0 + d) * a.data_stride;
+      if constexpr (CACHE_D) {
+        if (d != cur_d) {
+          if (a.data_cg) {   // data written earlier in the same launch
+#pragma unroll
+            for (int s = 0; s < 16; s++) {
+              float2 x = __ldcg(dp + t + T * s);
+              dreg[s] = {x.x, x.y};
+            }
+          } else {
+#pragma unroll
+            for (int s = 0; s < 16; s++) {
+              float2 x = __ldg(dp + t + T * s);
+              dreg[s] = {x.x, x.y};
+            }
+          }
+          cur_d = d;
+        }
 #pragma unroll
         for (int s = 0; s < 16; s++) {
-          float2 x = __ldg(dp + t + T * s);
-          dreg[s] = {x.x, x.y};
+          float2 h = __ldg(hp + t + T * s);
+          // D * conj(H)
+          v[s].x = fmaf(dreg[s].x, h.x, dreg[s].y * h.y);
+          v[s].y = fmaf(dreg[s].y, h.x, -dreg[s].x * h.y);
         }
-        cur_d = d;
-      }
-      const float2 *hp = a.tmpl + (long long)(a.t0 + tt) * a.tmpl_stride;
+      } else {
 #pragma unroll
-      for (int s = 0; s < 16; s++) {
-        float2 h = __ldg(hp + t + T * s);
-        // D * conj(H)
-        v[s].x = fmaf(dreg[s].x, h.x, dreg[s].y * h.y);
-        v[s].y = fmaf(dreg[s].y, h.x, -dreg[s].x * h.y);
+        for (int s = 0; s < 16; s++) {
+          const float2 x = a.data_cg ? __ldcg(dp + t + T * s) : __ldg(dp + t + T * s);
+          const float2 h = __ldg(hp + t + T * s);
+          v[s].x = fmaf(x.x, h.x, x.y * h.y);
+          v[s].y = fmaf(x.y, h.x, -x.x * h.y);
+        }
       }
     } else {
 #pragma unroll
@@ -467,6 +487,20 @@ flat_kernel(const FlatArgs a) {
       for (int b = t; b < nb; b += T) nxt[b] = 0ull;
     }
   }
+}
+
+template <int N, int MODE>
+__global__ void __launch_bounds__(FlatGeo<N>::CTA, FlatGeo<N>::CTA <= 256 ? 2 : 1)
+flat_kernel(const FlatArgs a) {
+  constexpr int G = FlatGeo<N>::G;
+  extern __shared__ __align__(16) float2 smem[];
+  // Work: dense block or a device list of output rows, split evenly.
+  const long long total = a.list ? (long long)(*a.list_count) : (long long)a.nd * a.nt;
+  const long long items = (total + G - 1) / G;
+  const long long per = items / gridDim.x, extra = items % gridDim.x;
+  const long long ibeg = blockIdx.x * per + (blockIdx.x < extra ? blockIdx.x : extra);
+  const long long iend = ibeg + per + (blockIdx.x < extra ? 1 : 0);
+  flat_range<N, MODE>(a, ibeg, iend, smem);
 }
 
 }  // namespace mfb

@@ -15,12 +15,16 @@
 #include <mutex>
 #include <map>
 #include <algorithm>
+#include <memory>
+#include <climits>
+#include <cstddef>
 #include "../../include/mfb.h"
 #include "flat_kernel.cuh"
 #include "series_kernel.cuh"
 #include "hier_kernels.cuh"
 #include "large_kernel.cuh"
 #include "adjoint_kernel.cuh"
+#include "batch_kernel.cuh"
 
 using namespace mfb;
 
@@ -1296,5 +1300,308 @@ extern "C" int mfb_adjoint(int device, size_t n, const void *data, int nd, const
                      (const float2 *)gz, (float2 *)grad_tmpl, *tw, sms, st);
     if (r) return r;
   }
+  return MFB_OK;
+}
+
+// ---------------------------------------------------------------- batched jobs
+struct mfb_batch {
+  int device = 0;
+  BatchArgs args;
+  void *arena = nullptr;          // jobs, segments, batch totals, counters
+  void *table = nullptr;          // device copy of the constant table (args + jobs)
+  size_t table_bytes = 0;
+  void *counters = nullptr;       // ticket, a_done, b_done, fwd_done, err: cleared every run
+  size_t counter_bytes = 0;
+  std::vector<std::pair<void *, size_t>> rec_clear;   // two-pass outputs, cleared every run
+  std::vector<void *> owned;      // series workspaces and block starts
+  float2 *slots = nullptr;
+  int grid = 0, smem = 0, nbatch = 0;
+  size_t scratch_bytes = 0;
+};
+
+static void batch_free(mfb_batch *b) {
+  if (!b) return;
+  DeviceGuard dg(b->device);
+  cudaFree(b->arena);
+  cudaFree(b->slots);
+  for (void *p : b->owned) cudaFree(p);
+  delete b;
+}
+
+extern "C" int mfb_batch_destroy(mfb_batch *b) {
+  batch_free(b);
+  return MFB_OK;
+}
+
+namespace {
+struct PendingBatch { int job, q_local, count; };
+}
+
+extern "C" int mfb_batch_create(mfb_batch **out, int device, const mfb_job *jobs, int njobs,
+                                const mfb_batch_opts *opts) {
+  if (!out) return fail(MFB_ERR_ARG, "null output handle");
+  *out = nullptr;
+  if (!jobs || njobs < 1) return fail(MFB_ERR_ARG, "no jobs");
+  if (njobs > BATCH_MAX_JOBS)
+    return fail(MFB_ERR_UNSUPPORTED, "%d jobs; one batch takes at most %d", njobs, BATCH_MAX_JOBS);
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(MFB_ERR_ARG, "no device %d", device);
+  const size_t slot_bytes = (opts && opts->slot_bytes) ? opts->slot_bytes : ((size_t)32 << 20);
+  const int nslots = (opts && opts->slots) ? opts->slots : 3;
+  if (nslots < 2 || nslots > 64) return fail(MFB_ERR_ARG, "slots must be 2 .. 64");
+  DeviceGuard dg(device);
+  std::unique_ptr<mfb_batch, void (*)(mfb_batch *)> b(new mfb_batch, batch_free);
+  b->device = device;
+  memset(&b->args, 0, sizeof b->args);
+  std::vector<BatchJob> hj(njobs);
+  bool any_two = false;
+  for (int i = 0; i < njobs; i++) {
+    const mfb_job &J = jobs[i];
+    BatchJob &j = hj[i];
+    memset(&j, 0, sizeof j);
+    const size_t n = J.n;
+    if (!mfb_supported(n)) return fail(MFB_ERR_UNSUPPORTED, "job %d: unsupported n=%zu", i, n);
+    if (J.nd < 1 || J.nt < 1) return fail(MFB_ERR_ARG, "job %d: nd and nt must be >= 1", i);
+    if (!J.templates || !J.records) return fail(MFB_ERR_ARG, "job %d: null templates or records", i);
+    if (((uintptr_t)J.records & 15u) != 0) return fail(MFB_ERR_ARG, "job %d: records not 16-byte aligned", i);
+    const bool series = J.series != nullptr;
+    if (series ? (!J.starts || J.nseries < 1) : !J.data)
+      return fail(MFB_ERR_ARG, "job %d: give data spectra, or series with block starts", i);
+    if (J.binsize < 1) return fail(MFB_ERR_ARG, "job %d: binsize must be >= 1", i);
+    if (std::isnan(J.threshold)) return fail(MFB_ERR_ARG, "job %d: threshold is NaN", i);
+    const size_t nb = mfb_nbins(n, J.binsize, J.start, J.end);
+    if (nb == 0) return fail(MFB_ERR_ARG, "job %d: empty window [%zu, %zu)", i, J.start, J.end);
+    j.n = (int)n; j.nd = J.nd; j.nt = J.nt; j.nb = (int)nb;
+    j.binsize = J.binsize > n ? (int)n : (int)J.binsize;
+    j.ws = (int)J.start;
+    j.we = (int)(J.end > n ? n : J.end);
+    j.t2 = J.threshold > 0.f ? J.threshold * J.threshold : 0.f;
+    j.tmpl = (const float2 *)J.templates;
+    j.rec = (uint4 *)J.records;
+    j.scale = 1.0f / (float)n;
+    j.fwd_ctr = i;
+    int L = 0;
+    while (((size_t)1 << L) < n) L++;
+    if (n <= 4096) {
+      NConst *c = nullptr;
+      int r = get_const(device, (int)n, &c);
+      if (r) return r;
+      j.twid = c->twid;
+      j.unit_items = J.unit_items > 0 ? J.unit_items : 1;
+    } else {
+      any_two = true;
+      const int N2 = J.split ? J.split : (n >= 16384 ? 256 : 128);
+      if (N2 != 64 && N2 != 128 && N2 != 256)
+        return fail(MFB_ERR_ARG, "job %d: split (N2) must be 64, 128 or 256", i);
+      const size_t N1 = n / (size_t)N2;
+      if (N1 < 64 || N1 > 4096)
+        return fail(MFB_ERR_UNSUPPORTED, "job %d: n=%zu with N2=%d gives N1=%zu outside 64 .. 4096",
+                    i, n, N2, N1);
+      if (nb > (size_t)BATCH_MAX_BINS)
+        return fail(MFB_ERR_UNSUPPORTED, "job %d: %zu bins per pair; n >= 8192 takes at most %d", i,
+                    nb, BATCH_MAX_BINS);
+      if (n * sizeof(float2) > slot_bytes)
+        return fail(MFB_ERR_ARG, "job %d: one pair (%zu bytes) does not fit a %zu-byte slot", i,
+                    n * sizeof(float2), slot_bytes);
+      j.N1 = (int)N1; j.N2 = N2;
+      NConst *c1 = nullptr, *c2 = nullptr;
+      AdjTables *tw = nullptr;
+      int r = get_const(device, (int)N1, &c1);
+      if (!r) r = get_const(device, N2, &c2);
+      if (!r) r = get_adj_tables(device, (int)n, &tw);
+      if (r) return r;
+      j.tw1 = c1->twid; j.tw2 = c2->twid;
+      j.tw_hi = tw->hi; j.tw_lo = tw->lo; j.lo_bits = tw->lo_bits;
+      j.batch_pairs = (int)std::max<size_t>(1, slot_bytes / (n * sizeof(float2)));
+      b->rec_clear.push_back({J.records, (size_t)J.nd * J.nt * nb * 16});
+    }
+    if (series) {
+      void *spec = nullptr, *st = nullptr;
+      CUDA_TRY(cudaMalloc(&spec, (size_t)J.nd * n * sizeof(float2)));
+      b->owned.push_back(spec);
+      CUDA_TRY(cudaMalloc(&st, (size_t)J.nd * sizeof(uint64_t)));
+      b->owned.push_back(st);
+      CUDA_TRY(cudaMemcpy(st, J.starts, (size_t)J.nd * sizeof(uint64_t), cudaMemcpyHostToDevice));
+      j.spec = (float2 *)spec;
+      j.data = (const float2 *)spec;
+      j.series = (const float2 *)J.series;
+      j.nseries = (long long)J.nseries;
+      j.starts = (const unsigned long long *)st;
+    } else {
+      j.data = (const float2 *)J.data;
+    }
+  }
+
+  // Segments: forward transforms first, then the two-pass pipeline, then the
+  // single-CTA jobs (largest n first), so every wait is on earlier tickets.
+  std::vector<BatchSeg> segs;
+  std::vector<unsigned> a_total, b_total;
+  long long t = 0;
+  auto add = [&](int job, int kind, int q, int q_local, long long units, int pairs) -> int {
+    if (units < 1) return MFB_OK;
+    if (units > INT32_MAX) return fail(MFB_ERR_UNSUPPORTED, "job %d: too many units", job);
+    BatchSeg s;
+    s.t0 = t; s.job = job; s.kind = kind; s.q = q; s.q_local = q_local;
+    s.units = (int)units; s.pairs = pairs;
+    segs.push_back(s);
+    t += units;
+    return MFB_OK;
+  };
+  for (int i = 0; i < njobs; i++) {
+    BatchJob &j = hj[i];
+    if (j.spec && j.n <= 4096) {
+      const int G = 4096 / j.n;
+      j.fwd_units = (j.nd + G - 1) / G;
+      int r = add(i, SEG_FWD_SMALL, 0, 0, j.fwd_units, 0);
+      if (r) return r;
+    }
+  }
+  int q = 0;
+  auto pipeline = [&](const std::vector<PendingBatch> &list, int kind_a, int kind_b) -> int {
+    const int q0 = q;
+    for (size_t k = 0; k < list.size(); k++) {
+      const BatchJob &j = hj[list[k].job];
+      const unsigned units = (unsigned)((long long)list[k].count * (j.n / 4096));
+      a_total.push_back(units);
+      b_total.push_back(units);
+      q++;
+    }
+    for (size_t k = 0; k <= list.size(); k++) {
+      if (k < list.size()) {
+        const PendingBatch &p = list[k];
+        int r = add(p.job, kind_a, q0 + (int)k, p.q_local, a_total[q0 + k], p.count);
+        if (r) return r;
+      }
+      if (k >= 1) {
+        const PendingBatch &p = list[k - 1];
+        int r = add(p.job, kind_b, q0 + (int)k - 1, p.q_local, b_total[q0 + k - 1], p.count);
+        if (r) return r;
+      }
+    }
+    return MFB_OK;
+  };
+  std::vector<PendingBatch> fwd_list, pair_list;
+  for (int i = 0; i < njobs; i++) {
+    BatchJob &j = hj[i];
+    if (j.n <= 4096) continue;
+    if (j.spec) {
+      for (int q_local = 0, b0 = 0; b0 < j.nd; q_local++, b0 += j.batch_pairs) {
+        const int c = std::min(j.batch_pairs, j.nd - b0);
+        fwd_list.push_back({i, q_local, c});
+        j.fwd_units += c * (j.n / 4096);
+      }
+    }
+    const long long pairs = (long long)j.nd * j.nt;
+    long long q_local = 0;
+    for (long long p0 = 0; p0 < pairs; p0 += j.batch_pairs, q_local++) {
+      if (q_local > INT32_MAX) return fail(MFB_ERR_UNSUPPORTED, "job %d: too many batches", i);
+      pair_list.push_back({i, (int)q_local, (int)std::min<long long>(j.batch_pairs, pairs - p0)});
+    }
+  }
+  int r = pipeline(fwd_list, SEG_FA, SEG_FB);
+  if (!r) r = pipeline(pair_list, SEG_A, SEG_B);
+  if (r) return r;
+  std::vector<int> small;
+  for (int i = 0; i < njobs; i++)
+    if (hj[i].n <= 4096) small.push_back(i);
+  std::stable_sort(small.begin(), small.end(), [&](int x, int y) { return hj[x].n > hj[y].n; });
+  for (int i : small) {
+    const BatchJob &j = hj[i];
+    const long long G = 4096 / j.n;
+    const long long items = ((long long)j.nd * j.nt + G - 1) / G;
+    r = add(i, SEG_SMALL, 0, 0, (items + j.unit_items - 1) / j.unit_items, 0);
+    if (r) return r;
+  }
+  if (segs.empty()) return fail(MFB_ERR_ARG, "no work");
+
+  // One arena: table (args + jobs) | segments | a_total | b_total | counters.
+  auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const int Q = (int)a_total.size();
+  b->table_bytes = offsetof(BatchTable, jobs) + njobs * sizeof(BatchJob);
+  const size_t o_jobs = 0, o_segs = up(b->table_bytes);
+  const size_t o_at = o_segs + up(segs.size() * sizeof(BatchSeg));
+  const size_t o_bt = o_at + up(Q * sizeof(unsigned) + 4);
+  const size_t o_ctr = o_bt + up(Q * sizeof(unsigned) + 4);
+  const size_t ctr_bytes = 8 + 2 * (size_t)Q * sizeof(unsigned) + (size_t)njobs * sizeof(unsigned) + 8;
+  CUDA_TRY(cudaMalloc(&b->arena, o_ctr + up(ctr_bytes)));
+  char *base = (char *)b->arena;
+  b->table = base + o_jobs;
+  CUDA_TRY(cudaMemcpy(base + o_segs, segs.data(), segs.size() * sizeof(BatchSeg),
+                      cudaMemcpyHostToDevice));
+  if (Q) {
+    CUDA_TRY(cudaMemcpy(base + o_at, a_total.data(), Q * sizeof(unsigned), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(base + o_bt, b_total.data(), Q * sizeof(unsigned), cudaMemcpyHostToDevice));
+  }
+  char *ctr = base + o_ctr;
+  b->counters = ctr;
+  b->counter_bytes = ctr_bytes;
+  BatchArgs &A = b->args;
+  A.segs = (const BatchSeg *)(base + o_segs);
+  A.nseg = (int)segs.size();
+  A.total = t;
+  A.ticket = (unsigned long long *)ctr;
+  A.a_done = (unsigned *)(ctr + 8);
+  A.b_done = A.a_done + Q;
+  A.fwd_done = A.b_done + Q;
+  A.err = (int *)(A.fwd_done + njobs);
+  A.a_total = (const unsigned *)(base + o_at);
+  A.b_total = (const unsigned *)(base + o_bt);
+  A.nslots = nslots;
+  A.slot_elems = (long long)(slot_bytes / sizeof(float2));
+  if (any_two) {
+    CUDA_TRY(cudaMalloc(&b->slots, (size_t)nslots * slot_bytes));
+    b->scratch_bytes = (size_t)nslots * slot_bytes;
+  }
+  A.slots = b->slots;
+  b->nbatch = Q;
+  {
+    std::vector<char> table(b->table_bytes);
+    memcpy(table.data() + offsetof(BatchTable, args), &A, sizeof A);
+    memcpy(table.data() + offsetof(BatchTable, jobs), hj.data(), njobs * sizeof(BatchJob));
+    CUDA_TRY(cudaMemcpy(b->table, table.data(), b->table_bytes, cudaMemcpyHostToDevice));
+  }
+  b->smem = batch_smem_bytes();
+  CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, b->smem));
+  int per_sm = 0, sms = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, BATCH_CTA, b->smem));
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  if (per_sm < 1) return fail(MFB_ERR_CUDA, "batched kernel cannot be resident");
+  b->grid = per_sm * sms;
+  *out = b.release();
+  return MFB_OK;
+}
+
+extern "C" int mfb_batch_run(mfb_batch *b, void *stream) {
+  if (!b) return fail(MFB_ERR_ARG, "null batch");
+  DeviceGuard dg(b->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyToSymbolAsync(c_batch, b->table, b->table_bytes, 0,
+                                    cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(b->counters, 0, b->counter_bytes, st));
+  for (auto &z : b->rec_clear) CUDA_TRY(cudaMemsetAsync(z.first, 0, z.second, st));
+  batch_kernel<<<b->grid, BATCH_CTA, b->smem, st>>>();
+  CUDA_TRY(cudaGetLastError());
+  return MFB_OK;
+}
+
+extern "C" int mfb_batch_status(mfb_batch *b, void *stream) {
+  if (!b) return fail(MFB_ERR_ARG, "null batch");
+  DeviceGuard dg(b->device);
+  CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  int err = 0;
+  CUDA_TRY(cudaMemcpy(&err, b->args.err, sizeof err, cudaMemcpyDeviceToHost));
+  if (err) return fail(MFB_ERR_CUDA, "batched launch stopped: a dependency wait ran out (code %d)", err);
+  return MFB_OK;
+}
+
+extern "C" int mfb_batch_info(mfb_batch *b, int64_t *tickets, int *grid, int *segments,
+                              int *batches, size_t *scratch_bytes) {
+  if (!b) return fail(MFB_ERR_ARG, "null batch");
+  if (tickets) *tickets = b->args.total;
+  if (grid) *grid = b->grid;
+  if (segments) *segments = b->args.nseg;
+  if (batches) *batches = b->nbatch;
+  if (scratch_bytes) *scratch_bytes = b->scratch_bytes;
   return MFB_OK;
 }

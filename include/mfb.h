@@ -152,6 +152,57 @@ int mfb_hier_config(mfb_hplan *p, size_t *band, int *coarse_kind);
 int mfb_hier_coarse_values(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t start,
                            size_t end, float *out);
 
+/* ---- batched uneven jobs --------------------------------------------------- */
+
+/* One job of a batch: a (data or series, templates) block of any supported n,
+   its own binsize, threshold and lag window (the same for every row). */
+typedef struct mfb_job {
+  size_t n;                 /* power of two, 64 ... 2^20 */
+  int nd, nt;               /* data rows (series blocks) and templates */
+  const void *data;         /* DEVICE complex64 [nd][n] spectra; NULL for a series job */
+  const void *templates;    /* DEVICE complex64 [nt][n] */
+  const void *series;       /* series job: DEVICE complex64 [nseries] samples, else NULL */
+  size_t nseries;
+  const uint64_t *starts;   /* series job: HOST [nd] block starts; block b is
+                               series[starts[b] .. starts[b]+n), zero past the end,
+                               transformed as FFT(x/n) (src/matchfilt.c:454-470) */
+  size_t binsize;
+  float threshold;
+  size_t start, end;        /* lag window, clamped to [0, n] */
+  void *records;            /* DEVICE output [nd][nt][nb] 16-byte records in PEAK_DTYPE
+                               layout {int64 index; complex64 value}, 16-byte aligned */
+  int split;                /* n >= 8192: N2 of the four-step split n = N1*N2, one of
+                               64, 128, 256 (0 = 256 for n >= 16384, else 128) */
+  int unit_items;           /* n <= 4096: items (of 4096/n pairs) per ticket (0 = 1) */
+} mfb_job;
+
+typedef struct mfb_batch_opts {
+  size_t slot_bytes;        /* two-pass scratch per slot (0 = 32 MiB) */
+  int slots;                /* scratch slots, 2 ... 64 (0 = 3) */
+} mfb_batch_opts;
+
+typedef struct mfb_batch mfb_batch;
+
+/* No single counterpart: the reference runs one plan per shape
+   (ap_mf_create / ap_mf_run, src/matchfilt.c:73-147,411-420; run_series,
+   src/matchfilt.c:437-490).  Plans a batch of jobs for ONE persistent launch:
+   validates every job, builds the twiddle tables, the segment table and the
+   scratch slots (allocates; do it before any capture).  Outputs are the
+   callers' `records`; inputs stay the callers' and must outlive the batch. */
+int mfb_batch_create(mfb_batch **out, int device, const mfb_job *jobs, int njobs,
+                     const mfb_batch_opts *opts);
+/* Clears the counters and the two-pass outputs and launches the persistent
+   kernel on `stream`.  No allocation, no host synchronisation: capturable
+   in a CUDA graph and replayable. */
+int mfb_batch_run(mfb_batch *b, void *stream);
+/* Synchronises `stream`; MFB_ERR_CUDA if a dependency wait inside the last
+   run ran out (the results of that run are then not valid). */
+int mfb_batch_status(mfb_batch *b, void *stream);
+/* Tickets, grid, segments, scratch batches and scratch bytes of the plan. */
+int mfb_batch_info(mfb_batch *b, int64_t *tickets, int *grid, int *segments, int *batches,
+                   size_t *scratch_bytes);
+int mfb_batch_destroy(mfb_batch *b);
+
 /* ---- adjoint --------------------------------------------------------------- */
 
 /* No counterpart in the reference (it has no gradients).  Adjoint of the peak
