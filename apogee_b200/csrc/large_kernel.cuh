@@ -178,6 +178,89 @@ large_pass_b(const LargeArgs a) {
   }
 }
 
+// Forward transforms of series blocks for n > 16384 (run_series): the same
+// two passes over block b = pair0 + bp of the series, conjugated and scaled by
+// 1/n on the way in (FFT(x) = conj(IFFT(conj(x)))), written back conjugated
+// in natural order: spectra row b, frequency N2*k1 + k2.
+struct LargeFwd {
+  const float2 *series;
+  long long nseries;
+  const unsigned long long *starts;   // [blocks]
+  float2 *spectra;                    // [blocks][n]
+  float scale;                        // 1/n
+};
+
+template <int N2>
+__global__ void __launch_bounds__(N2 >= 256 ? N2 : 256)
+large_fwd_a(const LargeArgs a, const LargeFwd s) {
+  constexpr int T2 = N2 / 16, C = LARGE_COLS;
+  extern __shared__ __align__(16) float2 smem[];
+  const int c = threadIdx.x % C, t = threadIdx.x / C;
+  float2 *buf = smem + c * FlatGeo<N2>::BUF;
+  const int tiles = a.N1 / C;
+  const long long work = (long long)a.batch * tiles;
+  const unsigned lo_mask = (1u << a.lo_bits) - 1u;
+  for (long long w = blockIdx.x; w < work; w += gridDim.x) {
+    const int bp = (int)(w / tiles), tile = (int)(w - (long long)bp * tiles);
+    const long long blk = a.pair0 + bp;
+    const int f1 = tile * C + c;
+    cf v[16];
+    if (blk < a.total) {
+      const long long s0 = (long long)s.starts[blk];
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        const long long e = s0 + f1 + (long long)a.N1 * (t + T2 * q);
+        float2 x = make_float2(0.f, 0.f);
+        if (e < s.nseries) x = __ldg(s.series + e);
+        v[q] = {x.x * s.scale, -x.y * s.scale};
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 16; q++) v[q] = {0.f, 0.f};
+    }
+    inverse_passes<N2, true>(v, buf, a.tw2, t);
+    float2 *yp = a.Y + (long long)bp * a.N2 * a.N1 + f1;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int k2 = t + T2 * q;
+      const unsigned m = ((unsigned)f1 * (unsigned)k2) & (unsigned)(a.n - 1);
+      const float2 wh = __ldg(a.tw_hi + (m >> a.lo_bits)), wl = __ldg(a.tw_lo + (m & lo_mask));
+      const cf y = cmul(v[q], cmul(cf{wh.x, wh.y}, cf{wl.x, wl.y}));
+      yp[(long long)k2 * a.N1] = make_float2(y.x, y.y);
+    }
+  }
+}
+
+template <int N1>
+__global__ void __launch_bounds__(FlatGeo<N1>::CTA)
+large_fwd_b(const LargeArgs a, const LargeFwd s) {
+  using Geo = FlatGeo<N1>;
+  constexpr int T1 = Geo::T, G = Geo::G;
+  extern __shared__ __align__(16) float2 smem[];
+  const int g = threadIdx.x / T1, t = threadIdx.x % T1;
+  float2 *buf = smem + g * Geo::BUF;
+  const long long work = (long long)a.batch * a.N2 / G;
+  for (long long w = blockIdx.x; w < work; w += gridDim.x) {
+    const long long r0 = w * G;
+    const int bp = (int)(r0 / a.N2), k2 = (int)(r0 - (long long)bp * a.N2) + g;
+    const long long blk = a.pair0 + bp;
+    const float2 *yp = a.Y + ((long long)bp * a.N2 + k2) * a.N1;
+    cf v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const float2 x = yp[t + T1 * q];
+      v[q] = {x.x, x.y};
+    }
+    inverse_passes<N1>(v, buf, a.tw1, t);
+    if (blk < a.total) {
+      float2 *o = s.spectra + blk * a.n + k2;
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        o[(long long)a.N2 * (t + T1 * q)] = make_float2(v[q].x, -v[q].y);
+    }
+  }
+}
+
 __global__ void large_finalize(const LargeArgs a) {
   const long long n_out = (long long)a.batch * a.nb;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_out;

@@ -201,6 +201,7 @@ static int large_a_attr(int *grid, int *smem, int *cta, int sms) {
   *smem = LARGE_COLS * FlatGeo<N2>::BUF * 8;
   *cta = N2;
   CUDA_TRY(cudaFuncSetAttribute(large_pass_a<N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
+  CUDA_TRY(cudaFuncSetAttribute(large_fwd_a<N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
   int b = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, large_pass_a<N2>, *cta, *smem));
   if (b < 1) return fail(MFB_ERR_CUDA, "large pass A (N2=%d) cannot be resident", N2);
@@ -212,6 +213,7 @@ static int large_b_attr(int *grid, int *smem, int *cta, int sms) {
   *smem = FlatGeo<N1>::G * FlatGeo<N1>::BUF * 8 + LARGE_MAX_BINS * 8;
   *cta = FlatGeo<N1>::CTA;
   CUDA_TRY(cudaFuncSetAttribute(large_pass_b<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
+  CUDA_TRY(cudaFuncSetAttribute(large_fwd_b<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
   int b = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, large_pass_b<N1>, *cta, *smem));
   if (b < 1) return fail(MFB_ERR_CUDA, "large pass B (N1=%d) cannot be resident", N1);
@@ -282,6 +284,24 @@ static cudaError_t launch_large(const LargeConst &c, const LargeArgs &a, cudaStr
   const long long outs = (long long)a.batch * a.nb;
   const int blocks = (int)std::min<long long>((outs + 255) / 256, 4096);
   large_finalize<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_large_fwd(const LargeConst &c, const LargeArgs &a, const LargeFwd &f,
+                                    cudaStream_t s) {
+  switch (c.N2) {
+    case 256: large_fwd_a<256><<<c.grid_a, c.cta_a, c.smem_a, s>>>(a, f); break;
+    case 512: large_fwd_a<512><<<c.grid_a, c.cta_a, c.smem_a, s>>>(a, f); break;
+    default: large_fwd_a<1024><<<c.grid_a, c.cta_a, c.smem_a, s>>>(a, f); break;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  switch (c.N1) {
+    case 128: large_fwd_b<128><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a, f); break;
+    case 256: large_fwd_b<256><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a, f); break;
+    case 512: large_fwd_b<512><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a, f); break;
+    default: large_fwd_b<1024><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a, f); break;
+  }
   return cudaGetLastError();
 }
 
@@ -431,12 +451,7 @@ static FlatArgs base_args(const mfb_plan *p, int d0, int nd, int t0, int nt, siz
 
 // Two-pass path for n > 16384.  list/nlist: listed output rows (host count),
 // or nullptr for the dense block.  Scratch is allocated on first use.
-static int run_large(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *list,
-                     long long nlist, size_t binsize, float threshold, size_t start, size_t end,
-                     size_t nb, int64_t *idx, void *val, int32_t *counts, int rs) {
-  if (nb > (size_t)LARGE_MAX_BINS)
-    return fail(MFB_ERR_UNSUPPORTED, "n=%zu supports at most %d bins per pair", p->n, LARGE_MAX_BINS);
-  const LargeConst &c = *p->lc;
+static int large_scratch(mfb_plan *p) {
   if (!p->lY) {
     const size_t per = p->n * sizeof(float2);
     int b = (int)std::max<size_t>(1, ((size_t)64 << 20) / per);
@@ -444,10 +459,23 @@ static int run_large(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t 
     CUDA_TRY(cudaMalloc(&p->lrec, (size_t)b * LARGE_MAX_BINS * sizeof(uint4)));
     p->lbatch = b;
   }
+  return MFB_OK;
+}
+
+// data: the rows to filter (default the plan's data rows).
+static int run_large(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *list,
+                     long long nlist, size_t binsize, float threshold, size_t start, size_t end,
+                     size_t nb, int64_t *idx, void *val, int32_t *counts, int rs,
+                     const float2 *data = nullptr) {
+  if (nb > (size_t)LARGE_MAX_BINS)
+    return fail(MFB_ERR_UNSUPPORTED, "n=%zu supports at most %d bins per pair", p->n, LARGE_MAX_BINS);
+  const LargeConst &c = *p->lc;
+  int sr = large_scratch(p);
+  if (sr) return sr;
   if (end > p->n) end = p->n;
   LargeArgs a;
   memset(&a, 0, sizeof a);
-  a.data = p->data;
+  a.data = data ? data : p->data;
   a.tmpl = p->tmpl;
   a.n = (int)p->n; a.N1 = c.N1; a.N2 = c.N2;
   a.d0 = d0; a.nd = nd; a.t0 = t0; a.nt = nt;
@@ -555,11 +583,33 @@ extern "C" int mfb_run_rows(mfb_plan *p, int d0, int nd, int t0, int nt, const i
 extern "C" int mfb_forward(mfb_plan *p, const void *series, size_t nseries,
                            const uint64_t *starts_dev, int nblocks, void *spectra) {
   if (!p) return fail(MFB_ERR_ARG, "null plan");
-  if (is_large(p->n))
-    return fail(MFB_ERR_UNSUPPORTED, "block forward transforms are built for n <= 16384");
   if (!series || !starts_dev || !spectra || nblocks < 1)
     return fail(MFB_ERR_ARG, "invalid forward-transform arguments");
   DeviceGuard dg(p->device);
+  if (is_large(p->n)) {
+    int sr = large_scratch(p);
+    if (sr) return sr;
+    const LargeConst &c = *p->lc;
+    LargeArgs a;
+    memset(&a, 0, sizeof a);
+    a.n = (int)p->n; a.N1 = c.N1; a.N2 = c.N2;
+    a.total = nblocks;
+    a.Y = p->lY;
+    a.tw1 = c.c1->twid; a.tw2 = c.c2->twid;
+    a.tw_hi = c.tw_hi; a.tw_lo = c.tw_lo; a.lo_bits = c.lo_bits;
+    LargeFwd f;
+    f.series = (const float2 *)series;
+    f.nseries = (long long)nseries;
+    f.starts = (const unsigned long long *)starts_dev;
+    f.spectra = (float2 *)spectra;
+    f.scale = 1.0f / (float)p->n;
+    for (long long p0 = 0; p0 < nblocks; p0 += p->lbatch) {
+      a.pair0 = p0;
+      a.batch = (int)std::min<long long>(p->lbatch, nblocks - p0);
+      CUDA_TRY(launch_large_fwd(c, a, f, p->stream));
+    }
+    return MFB_OK;
+  }
   SeriesArgs s;
   s.series = (const float2 *)series;
   s.nseries = (long long)nseries;
@@ -625,6 +675,14 @@ extern "C" int mfb_run_series(mfb_plan *p, const void *series, size_t nseries,
     int r = mfb_forward(p, series, nseries, p->starts_dev + b0, g, p->sspec);
     if (r) return r;
     size_t lo = win_start[b0], hi = win_end[b0];
+    if (is_large(p->n)) {
+      r = run_large(p, 0, g, t0, nt, nullptr, 0, binsize, threshold, lo, hi, nb0,
+                    idx + (size_t)b0 * nt * nb0, (float2 *)val + (size_t)b0 * nt * nb0,
+                    counts ? counts + (size_t)b0 * nt : nullptr, 1, p->sspec);
+      if (r) return r;
+      b0 += g;
+      continue;
+    }
     FlatArgs a = base_args(p, 0, g, t0, nt, binsize, threshold, lo, hi, nb0);
     a.data = p->sspec;
     a.out_idx = (long long *)idx + (size_t)b0 * nt * nb0;

@@ -90,3 +90,26 @@ def test_large_hierarchical_refine_is_flat():
     b = hf.run(binsize=n // 16)
     np.testing.assert_array_equal(a, b)
     assert hf.stats == (nd * nt, nd * nt)
+
+
+@pytest.mark.parametrize("n", [32768, 131072])
+def test_large_run_series(n):
+    """run_series for n > 16384: two-pass forward transforms of the blocks,
+    then the two-pass filter, grouped by window (src/matchfilt.c:437-490)."""
+    mf = _mf()
+    rng = np.random.default_rng(n + 7)
+    nt = 3
+    H = noise(rng, (nt, n))
+    series = rng.standard_normal(3 * n + n // 3).astype(np.float32)
+    starts = np.array([0, n // 2, n, 2 * n, 3 * n])          # the last one runs past the end
+    ws = np.array([n // 8, n // 8, 0, n // 8, n // 8])
+    we = np.array([n, n, n - n // 8, n, n])
+    f = mf.MatchedFilter(n, 2, nt)
+    f.set_templates(H)
+    bs = n // 32
+    idx, val = f.run_series(series.astype(np.complex64), starts, ws, we, binsize=bs, raw=True)
+    z = oracle.correlate(oracle.series_spectra(series, starts, n), H)
+    for b in range(starts.size):
+        bad = parity.compare(idx[b:b + 1], val[b:b + 1], z[b:b + 1], bs, 0.0,
+                             (int(ws[b]), int(we[b])))
+        assert not bad, (b, bad[:3])
