@@ -111,7 +111,7 @@ class BatchedFilter:
 
     tune : False (defaults), True (autotune every distinct n, cached per
            device), or a dict {n: {"split": N2} | {"unit_items": k}}.
-    slot_bytes, slots : scratch of the large-n four-step (0 = 32 MiB x 3).
+    slot_bytes, slots : scratch of the large-n four-step (0 = 64 MiB x 3).
     """
 
     def __init__(self, jobs, device=None, tune=False, slot_bytes=0, slots=0):

@@ -72,8 +72,10 @@ struct BatchSeg {
   int job, kind;
   int q;                              // global batch (slot user) index, SEG_A/B/FA/FB
   int q_local;                        // batch index inside the job
-  int units;
+  int units;                          // tickets
   int pairs;                          // pairs (blocks) in this batch
+  int raw;                            // A/B/FA/FB: work units (4096 points each)
+  int per;                            // A/B/FA/FB: work units per ticket
 };
 
 struct BatchArgs {
@@ -131,13 +133,13 @@ __device__ __forceinline__ bool batch_wait(const unsigned *ctr, unsigned target,
   return s_ok != 0;
 }
 
-// Publish this unit's global writes and count it; true for every thread of
-// the CTA when it was the last of `total` units counted on ctr.
-__device__ __forceinline__ bool batch_done(unsigned *ctr, unsigned total) {
+// Publish this ticket's global writes and count its `count` units; true for
+// every thread of the CTA when they were the last of `total` counted on ctr.
+__device__ __forceinline__ bool batch_done(unsigned *ctr, unsigned total, unsigned count = 1u) {
   __shared__ int s_last;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(ctr, 1u) == total - 1u);
+  if (threadIdx.x == 0) s_last = (atomicAdd(ctr, count) == total - count);
   __syncthreads();
   return s_last != 0;
 }
@@ -227,9 +229,11 @@ __device__ __noinline__ void a_unit(int jid, int segi, int u, float2 *smem) {
   if (!FWD && j.fwd_units && !batch_wait(a.fwd_done + j.fwd_ctr, (unsigned)j.fwd_units, a.err))
     return;
   const int c = threadIdx.x % C, t = threadIdx.x / C;
-  float2 *buf = smem + c * FlatGeo<N2>::BUF;
+  float2 *buf = smem + c * col_buf<N2>();
   const int tiles = j.N1 / C;
-  const int bp = u / tiles, tile = u - bp * tiles;
+  const int w0 = u * sg.per, w1 = min(sg.raw, w0 + sg.per);
+  for (int w = w0; w < w1; w++) {
+  const int bp = w / tiles, tile = w - bp * tiles;
   const long long pi = (long long)sg.q_local * j.batch_pairs + bp;
   const int f1 = tile * C + c;
   cf v[16];
@@ -266,7 +270,8 @@ __device__ __noinline__ void a_unit(int jid, int segi, int u, float2 *smem) {
     const cf y = cmul(v[q], cmul(cf{wh.x, wh.y}, cf{wl.x, wl.y}));
     yp[(long long)k2 * j.N1] = make_float2(y.x, y.y);
   }
-  batch_done(a.a_done + sg.q, a.a_total[sg.q]);
+  }
+  batch_done(a.a_done + sg.q, a.a_total[sg.q], (unsigned)(w1 - w0));
 }
 
 // Row pass: G1 = 4096/N1 rows k2 of one pair (or block), the N1-point inverse
@@ -284,7 +289,10 @@ __device__ __noinline__ void b_unit(int jid, int segi, int u, float2 *smem) {
   float2 *buf = smem + g * Geo::BUF;
   unsigned long long *keys = reinterpret_cast<unsigned long long *>(smem + G1 * Geo::BUF);
   const int rgroups = j.N2 / G1;
-  const int bp = u / rgroups, rg = u - bp * rgroups;
+  const int w0 = u * sg.per, w1 = min(sg.raw, w0 + sg.per);
+  for (int w = w0; w < w1; w++) {
+  __syncthreads();   // the previous unit's readers of keys and rows are done
+  const int bp = w / rgroups, rg = w - bp * rgroups;
   const int k2base = rg * G1, k2 = k2base + g;
   const long long pi = (long long)sg.q_local * j.batch_pairs + bp;
   const float2 *yp = a.slots + (long long)(sg.q % a.nslots) * a.slot_elems +
@@ -304,11 +312,7 @@ __device__ __noinline__ void b_unit(int jid, int segi, int u, float2 *smem) {
 #pragma unroll
     for (int q = 0; q < 16; q++)
       o[(long long)j.N2 * (t + T1 * q)] = make_float2(v[q].x, -v[q].y);
-    batch_done(a.b_done + sg.q, a.b_total[sg.q]);
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(a.fwd_done + j.fwd_ctr, 1u);
-    return;
+    continue;
   }
   int row, d, tt;
   batch_pair(j, pi, row, d, tt);
@@ -335,7 +339,13 @@ __device__ __noinline__ void b_unit(int jid, int segi, int u, float2 *smem) {
     rec_max(rec + b, make_uint4(__float_as_uint(val.x), __float_as_uint(val.y), (unsigned)kk,
                                 (unsigned)(kk >> 32)));
   }
-  if (batch_done(a.b_done + sg.q, a.b_total[sg.q])) {
+  }
+  if (FWD) {
+    batch_done(a.b_done + sg.q, a.b_total[sg.q], (unsigned)(w1 - w0));
+    if (threadIdx.x == 0) atomicAdd(a.fwd_done + j.fwd_ctr, (unsigned)(w1 - w0));
+    return;
+  }
+  if (batch_done(a.b_done + sg.q, a.b_total[sg.q], (unsigned)(w1 - w0))) {
     // Last row unit of the batch: records {re, im, ~lag, |z|^2 bits} become
     // {int64 index, re, im}, or {-1, 0, 0} where nothing was reported.
     const long long n_out = (long long)sg.pairs * j.nb;
@@ -471,9 +481,9 @@ constexpr int batch_smem_bytes() {
                         FlatGeo<512>::SMEM, FlatGeo<1024>::SMEM, FlatGeo<2048>::SMEM,
                         FlatGeo<4096>::SMEM};
   for (int i = 0; i < 7; i++) m = small[i] > m ? small[i] : m;
-  const int a_units[3] = {(BATCH_CTA / 4) * FlatGeo<64>::BUF * 8,
-                          (BATCH_CTA / 8) * FlatGeo<128>::BUF * 8,
-                          (BATCH_CTA / 16) * FlatGeo<256>::BUF * 8};
+  const int a_units[3] = {(BATCH_CTA / 4) * col_buf<64>() * 8,
+                          (BATCH_CTA / 8) * col_buf<128>() * 8,
+                          (BATCH_CTA / 16) * col_buf<256>() * 8};
   for (int i = 0; i < 3; i++) m = a_units[i] > m ? a_units[i] : m;
   const int b_units[7] = {FlatGeo<64>::G * FlatGeo<64>::BUF, FlatGeo<128>::G * FlatGeo<128>::BUF,
                           FlatGeo<256>::G * FlatGeo<256>::BUF, FlatGeo<512>::G * FlatGeo<512>::BUF,

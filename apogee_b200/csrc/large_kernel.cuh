@@ -27,7 +27,14 @@
 namespace mfb {
 
 constexpr int LARGE_MAX_BINS = 4096;
+constexpr int LARGE_SMALL_BINS = 512;   // pass-B launches with this many key slots or fewer
 constexpr int LARGE_COLS = 16;          // columns per pass-A CTA
+
+// Shared-memory stride between the column buffers of a pass-A CTA: one float2
+// more than a column needs, so that the same offset in consecutive columns
+// (what the threads of a half-warp touch together) falls in distinct banks.
+template <int N2>
+__host__ __device__ constexpr int col_buf() { return FlatGeo<N2>::BUF + 1; }
 
 struct LargeArgs {
   const float2 *data, *tmpl;            // rows of n complex64
@@ -71,7 +78,7 @@ large_pass_a(const LargeArgs a) {
   static_assert(T2 * C == N2, "pass A runs one thread per (column, point group)");
   extern __shared__ __align__(16) float2 smem[];
   const int c = threadIdx.x % C, t = threadIdx.x / C;
-  float2 *buf = smem + c * FlatGeo<N2>::BUF;
+  float2 *buf = smem + c * col_buf<N2>();
   const int tiles = a.N1 / C;
   const long long work = (long long)a.batch * tiles;
   const unsigned lo_mask = (1u << a.lo_bits) - 1u;
@@ -110,17 +117,25 @@ large_pass_a(const LargeArgs a) {
   }
 }
 
-// 128-bit max on the high 64 bits (the key); the low 64 bits (value) travel with it.
+// 128-bit max on the high 64 bits (the key); the low 64 bits (value) travel
+// with it.  Keys only grow, so a key already >= ours settles it with one plain
+// (single-copy atomic, 64-bit) read; otherwise compare-and-swap from the key
+// and value read separately -- if they were inconsistent the first swap fails
+// and returns the true record.
 __device__ __forceinline__ void rec_max(uint4 *slot, uint4 mine) {
+  const unsigned long long mkey = ((unsigned long long)mine.w << 32) | mine.z;
+  const unsigned long long *q = reinterpret_cast<const unsigned long long *>(slot);
+  const unsigned long long k0 = __ldcg(q + 1);
+  if (k0 >= mkey) return;
   unsigned __int128 *p = reinterpret_cast<unsigned __int128 *>(slot);
-  const unsigned __int128 m = ((unsigned __int128)(((unsigned long long)mine.w << 32) | mine.z) << 64) |
+  const unsigned __int128 m = ((unsigned __int128)mkey << 64) |
                               (((unsigned long long)mine.y << 32) | mine.x);
-  const unsigned long long mkey = (unsigned long long)(m >> 64);
-  unsigned __int128 old = atomicCAS(p, (unsigned __int128)0, (unsigned __int128)0);  // atomic read
-  while ((unsigned long long)(old >> 64) < mkey) {
+  unsigned __int128 old = ((unsigned __int128)k0 << 64) | __ldcg(q);
+  for (;;) {
     const unsigned __int128 prev = atomicCAS(p, old, m);
     if (prev == old) break;
     old = prev;
+    if ((unsigned long long)(old >> 64) >= mkey) break;
   }
 }
 
@@ -196,7 +211,7 @@ large_fwd_a(const LargeArgs a, const LargeFwd s) {
   constexpr int T2 = N2 / 16, C = LARGE_COLS;
   extern __shared__ __align__(16) float2 smem[];
   const int c = threadIdx.x % C, t = threadIdx.x / C;
-  float2 *buf = smem + c * FlatGeo<N2>::BUF;
+  float2 *buf = smem + c * col_buf<N2>();
   const int tiles = a.N1 / C;
   const long long work = (long long)a.batch * tiles;
   const unsigned lo_mask = (1u << a.lo_bits) - 1u;

@@ -193,12 +193,13 @@ struct LargeConst {
   float2 *tw_hi = nullptr, *tw_lo = nullptr;
   NConst *c1 = nullptr, *c2 = nullptr;
   int grid_a = 0, grid_b = 0, smem_a = 0, smem_b = 0, cta_a = 0, cta_b = 0;
+  int grid_bs = 0, smem_bs = 0;   // pass B with at most LARGE_SMALL_BINS keys
 };
 static std::map<std::pair<int, int>, LargeConst> g_large;
 
 template <int N2>
 static int large_a_attr(int *grid, int *smem, int *cta, int sms) {
-  *smem = LARGE_COLS * FlatGeo<N2>::BUF * 8;
+  *smem = LARGE_COLS * col_buf<N2>() * 8;
   *cta = N2;
   CUDA_TRY(cudaFuncSetAttribute(large_pass_a<N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
   CUDA_TRY(cudaFuncSetAttribute(large_fwd_a<N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
@@ -209,15 +210,19 @@ static int large_a_attr(int *grid, int *smem, int *cta, int sms) {
   return MFB_OK;
 }
 template <int N1>
-static int large_b_attr(int *grid, int *smem, int *cta, int sms) {
-  *smem = FlatGeo<N1>::G * FlatGeo<N1>::BUF * 8 + LARGE_MAX_BINS * 8;
-  *cta = FlatGeo<N1>::CTA;
-  CUDA_TRY(cudaFuncSetAttribute(large_pass_b<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
-  CUDA_TRY(cudaFuncSetAttribute(large_fwd_b<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
-  int b = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, large_pass_b<N1>, *cta, *smem));
-  if (b < 1) return fail(MFB_ERR_CUDA, "large pass B (N1=%d) cannot be resident", N1);
-  *grid = b * sms;
+static int large_b_attr(LargeConst &c, int sms) {
+  const int rows = FlatGeo<N1>::G * FlatGeo<N1>::BUF * 8;
+  c.smem_b = rows + LARGE_MAX_BINS * 8;
+  c.smem_bs = rows + LARGE_SMALL_BINS * 8;
+  c.cta_b = FlatGeo<N1>::CTA;
+  CUDA_TRY(cudaFuncSetAttribute(large_pass_b<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_b));
+  CUDA_TRY(cudaFuncSetAttribute(large_fwd_b<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_b));
+  int b = 0, bs = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, large_pass_b<N1>, c.cta_b, c.smem_b));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, large_pass_b<N1>, c.cta_b, c.smem_bs));
+  if (b < 1 || bs < 1) return fail(MFB_ERR_CUDA, "large pass B (N1=%d) cannot be resident", N1);
+  c.grid_b = b * sms;
+  c.grid_bs = bs * sms;
   return MFB_OK;
 }
 
@@ -253,10 +258,10 @@ static int get_large(int device, int n, LargeConst **out) {
   }
   if (r) return r;
   switch (c.N1) {
-    case 128: r = large_b_attr<128>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
-    case 256: r = large_b_attr<256>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
-    case 512: r = large_b_attr<512>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
-    case 1024: r = large_b_attr<1024>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
+    case 128: r = large_b_attr<128>(c, sms); break;
+    case 256: r = large_b_attr<256>(c, sms); break;
+    case 512: r = large_b_attr<512>(c, sms); break;
+    case 1024: r = large_b_attr<1024>(c, sms); break;
     default: return fail(MFB_ERR_UNSUPPORTED, "no four-step split for n=%d", n);
   }
   if (r) return r;
@@ -273,11 +278,13 @@ static cudaError_t launch_large(const LargeConst &c, const LargeArgs &a, cudaStr
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  const bool few = a.nb <= LARGE_SMALL_BINS;
+  const int gb = few ? c.grid_bs : c.grid_b, sb = few ? c.smem_bs : c.smem_b;
   switch (c.N1) {
-    case 128: large_pass_b<128><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a); break;
-    case 256: large_pass_b<256><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a); break;
-    case 512: large_pass_b<512><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a); break;
-    default: large_pass_b<1024><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a); break;
+    case 128: large_pass_b<128><<<gb, c.cta_b, sb, s>>>(a); break;
+    case 256: large_pass_b<256><<<gb, c.cta_b, sb, s>>>(a); break;
+    case 512: large_pass_b<512><<<gb, c.cta_b, sb, s>>>(a); break;
+    default: large_pass_b<1024><<<gb, c.cta_b, sb, s>>>(a); break;
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -297,10 +304,10 @@ static cudaError_t launch_large_fwd(const LargeConst &c, const LargeArgs &a, con
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   switch (c.N1) {
-    case 128: large_fwd_b<128><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a, f); break;
-    case 256: large_fwd_b<256><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a, f); break;
-    case 512: large_fwd_b<512><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a, f); break;
-    default: large_fwd_b<1024><<<c.grid_b, c.cta_b, c.smem_b, s>>>(a, f); break;
+    case 128: large_fwd_b<128><<<c.grid_bs, c.cta_b, c.smem_bs, s>>>(a, f); break;
+    case 256: large_fwd_b<256><<<c.grid_bs, c.cta_b, c.smem_bs, s>>>(a, f); break;
+    case 512: large_fwd_b<512><<<c.grid_bs, c.cta_b, c.smem_bs, s>>>(a, f); break;
+    default: large_fwd_b<1024><<<c.grid_bs, c.cta_b, c.smem_bs, s>>>(a, f); break;
   }
   return cudaGetLastError();
 }
@@ -1165,9 +1172,9 @@ static int static_setup(int device, StaticDev **out) {
       }
       if (r) break;
       switch (c.N1) {
-        case 128: r = large_b_attr<128>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
-        case 256: r = large_b_attr<256>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
-        default: r = large_b_attr<512>(&c.grid_b, &c.smem_b, &c.cta_b, sms); break;
+        case 128: r = large_b_attr<128>(c, sms); break;
+        case 256: r = large_b_attr<256>(c, sms); break;
+        default: r = large_b_attr<512>(c, sms); break;
       }
     }
     if (r) return r;
@@ -1405,7 +1412,7 @@ extern "C" int mfb_batch_create(mfb_batch **out, int device, const mfb_job *jobs
   int ndev = 0;
   CUDA_TRY(cudaGetDeviceCount(&ndev));
   if (device < 0 || device >= ndev) return fail(MFB_ERR_ARG, "no device %d", device);
-  const size_t slot_bytes = (opts && opts->slot_bytes) ? opts->slot_bytes : ((size_t)32 << 20);
+  const size_t slot_bytes = (opts && opts->slot_bytes) ? opts->slot_bytes : ((size_t)64 << 20);
   const int nslots = (opts && opts->slots) ? opts->slots : 3;
   if (nslots < 2 || nslots > 64) return fail(MFB_ERR_ARG, "slots must be 2 .. 64");
   DeviceGuard dg(device);
@@ -1496,14 +1503,29 @@ extern "C" int mfb_batch_create(mfb_batch **out, int device, const mfb_job *jobs
   std::vector<BatchSeg> segs;
   std::vector<unsigned> a_total, b_total;
   long long t = 0;
+  // Grid first: A/B tickets take several work units when a segment has
+  // enough of them to keep every CTA busy for two tickets.
+  const int smem = batch_smem_bytes();
+  CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0, sms = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, BATCH_CTA, smem));
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  if (per_sm < 1) return fail(MFB_ERR_CUDA, "batched kernel cannot be resident");
+  const long long grid = (long long)per_sm * sms;
   auto add = [&](int job, int kind, int q, int q_local, long long units, int pairs) -> int {
     if (units < 1) return MFB_OK;
     if (units > INT32_MAX) return fail(MFB_ERR_UNSUPPORTED, "job %d: too many units", job);
     BatchSeg s;
+    memset(&s, 0, sizeof s);
     s.t0 = t; s.job = job; s.kind = kind; s.q = q; s.q_local = q_local;
-    s.units = (int)units; s.pairs = pairs;
+    s.pairs = pairs;
+    s.raw = (int)units;
+    s.per = 1;
+    if (kind != SEG_SMALL && kind != SEG_FWD_SMALL)
+      s.per = (int)std::max<long long>(1, std::min<long long>(8, units / (2 * grid)));
+    s.units = (int)((units + s.per - 1) / s.per);
     segs.push_back(s);
-    t += units;
+    t += s.units;
     return MFB_OK;
   };
   for (int i = 0; i < njobs; i++) {
@@ -1619,13 +1641,8 @@ extern "C" int mfb_batch_create(mfb_batch **out, int device, const mfb_job *jobs
     memcpy(table.data() + offsetof(BatchTable, jobs), hj.data(), njobs * sizeof(BatchJob));
     CUDA_TRY(cudaMemcpy(b->table, table.data(), b->table_bytes, cudaMemcpyHostToDevice));
   }
-  b->smem = batch_smem_bytes();
-  CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, b->smem));
-  int per_sm = 0, sms = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, BATCH_CTA, b->smem));
-  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  if (per_sm < 1) return fail(MFB_ERR_CUDA, "batched kernel cannot be resident");
-  b->grid = per_sm * sms;
+  b->smem = smem;
+  b->grid = (int)grid;
   *out = b.release();
   return MFB_OK;
 }

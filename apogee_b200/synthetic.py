@@ -104,3 +104,49 @@ def hier_workload(n=4096, nd=16, nt=1024, seed=1, frac=0.10, snr_lo=5.0, snr_hi=
         inj.append((int(d), t, lag, snr))
     power = (np.abs(H.astype(np.complex128)) ** 2).mean(0).astype(np.float32)
     return D.astype(np.complex64), H, power, inj
+
+
+def batched_workload(njobs=256, seed=2, device="cuda", nmin_log=10, nmax_log=16, nd_max=64,
+                     nt_min=16, nt_max=4096, cap_bytes=2 << 30, series_every=4, inject_every=8,
+                     snr=8.0):
+    """Uneven jobs for the batched launch, generated on the device.
+
+    Job i: n = 2^U{nmin_log..nmax_log}, nd ~ U{1..nd_max}, nt ~ U{nt_min..nt_max}
+    capped so that nt*n*8 <= cap_bytes, binsize n/16 or n/64; templates by the
+    template_bank formula (bins 20..n/2-1) drawn from the seed; every
+    `series_every`-th job is a series job (float32 N(0,1) samples cut into nd
+    back-to-back blocks of n), the others take noise spectra (FFT of N(0,1)
+    / sqrt(n)) with every `inject_every`-th row carrying a template at a
+    random lag and SNR `snr`.  Returns a list of batch.Job on `device`.
+    """
+    import torch
+    from .batch import Job
+    rng = np.random.default_rng(seed)
+    dev = torch.device(device)
+    gen = torch.Generator(device=dev).manual_seed(seed)
+    jobs = []
+    for i in range(njobs):
+        n = 1 << int(rng.integers(nmin_log, nmax_log + 1))
+        nd = int(rng.integers(1, nd_max + 1))
+        nt = int(min(rng.integers(nt_min, nt_max + 1), cap_bytes // (8 * n)))
+        binsize = n // int(rng.choice([16, 64]))
+        alpha = torch.tensor(rng.uniform(1e2, 1e4, size=nt), dtype=torch.float64, device=dev)
+        tc = torch.tensor(rng.uniform(0, n, size=nt), dtype=torch.float64, device=dev)
+        H = torch.empty(nt, n, dtype=torch.complex64, device=dev)
+        chunk = max(1, (1 << 25) // n)
+        for t0 in range(0, nt, chunk):
+            H[t0:t0 + chunk] = template_bank_torch(n, alpha[t0:t0 + chunk],
+                                                   tc[t0:t0 + chunk]).to(torch.complex64)
+        if series_every and i % series_every == series_every - 1:
+            x = torch.randn(nd * n, dtype=torch.float32, device=dev, generator=gen)
+            jobs.append(Job(H, series=x, starts=np.arange(nd) * n, binsize=binsize))
+        else:
+            D = torch.fft.fft(torch.randn(nd, n, dtype=torch.float32, device=dev, generator=gen),
+                              dim=1) / float(np.sqrt(n))
+            k = torch.arange(n, device=dev, dtype=torch.float64)
+            for d in range(0, nd, inject_every):
+                t, lag = int(rng.integers(nt)), int(rng.integers(n))
+                D[d] += (snr * H[t].to(torch.complex128) *
+                         torch.exp(-2j * np.pi * k * lag / n)).to(torch.complex64)
+            jobs.append(Job(H, data=D.to(torch.complex64).contiguous(), binsize=binsize))
+    return jobs

@@ -53,7 +53,8 @@ typedef struct mfb_hplan mfb_hplan;
 /* ---- flat matched filter ------------------------------------------------ */
 
 /* Replaces ap_mf_create (src/matchfilt.c:73-133; matchedfilter.h:53).  n is a
-   power of two, 64..16384; device is a CUDA ordinal.  *out = NULL on error. */
+   power of two, 64 .. 2^20 (above 16384 the two-pass four-step); device is a
+   CUDA ordinal.  *out = NULL on error. */
 int mfb_create(mfb_plan **out, size_t n, int ndata, int ntmpl, int device);
 /* Replaces ap_mf_destroy (src/matchfilt.c:135-146). */
 int mfb_destroy(mfb_plan *p);
@@ -177,7 +178,7 @@ typedef struct mfb_job {
 } mfb_job;
 
 typedef struct mfb_batch_opts {
-  size_t slot_bytes;        /* two-pass scratch per slot (0 = 32 MiB) */
+  size_t slot_bytes;        /* two-pass scratch per slot (0 = 64 MiB) */
   int slots;                /* scratch slots, 2 ... 64 (0 = 3) */
 } mfb_batch_opts;
 
