@@ -410,9 +410,9 @@ class MatchedFilter:
         st = np.ascontiguousarray(layout.starts, dtype=np.uint64)
         lo = np.ascontiguousarray(layout.low, dtype=np.uint64)
         hi = np.ascontiguousarray(layout.high, dtype=np.uint64)
-        rc = _lib.lib().mfb_run_series(self._plan, ser.data_ptr(), ser.numel(), st.ctypes.data,
-                                       lo.ctypes.data, hi.ctypes.data, nblk, t0, nt, binsize,
-                                       threshold, idx_d.data_ptr(), val_d.data_ptr(), None)
+        rc = self._series_call(ser.data_ptr(), ser.numel(), st.ctypes.data, lo.ctypes.data,
+                               hi.ctypes.data, nblk, t0, nt, binsize, threshold,
+                               idx_d.data_ptr(), val_d.data_ptr())
         _lib.check(rc, "run_series failed")
         idx = idx_d.cpu().numpy().reshape(nblk, nt, nb)
         val = val_d.cpu().numpy().reshape(nblk, nt, nb)
@@ -427,6 +427,9 @@ class MatchedFilter:
         out = np.empty(idx.shape, PEAK_DTYPE)
         out["index"], out["value"] = idx, val
         return out
+
+    def _series_call(self, *args):
+        return _lib.lib().mfb_run_series(self._plan, *args, None)
 
     # ---- compatibility ----------------------------------------------------------
     def empty_shared(self, shape, dtype=np.complex64):
@@ -786,9 +789,26 @@ class HierarchicalFilter(MatchedFilter):
                                                      out.data_ptr()))
         return out.cpu().numpy().reshape(nd, nt)
 
-    def run_series(self, *a, **k):
-        raise NotImplementedError("run_series on HierarchicalFilter is not built yet; "
-                                  "use MatchedFilter.run_series")
+    def run_series(self, series, starts, win_start, win_end,
+                   binsize=None, threshold=0.0, templates=None, raw=False):
+        """Hierarchical filter over a caller-supplied block layout
+        (ap_hmf_run_series, src/hmf.c:158-220): runs of blocks with equal
+        windows, at most ndata at a time, are transformed on the device into
+        the plan's data rows and run through coarse pass, gate and refine.
+        The data set with set_data() is restored before the next run()."""
+        self._prepare()
+        kept = (self._dataset,
+                None if self._data_ready is None else set(self._data_ready))
+        try:
+            return MatchedFilter.run_series(self, series, starts, win_start, win_end,
+                                            binsize=binsize, threshold=threshold,
+                                            templates=templates, raw=raw)
+        finally:
+            self._dataset, self._data_ready = kept
+            self._ddirty = True
+
+    def _series_call(self, *args):
+        return _lib.lib().mfb_hier_run_series(self._hplan, *args, None)
 
     @property
     def config(self):

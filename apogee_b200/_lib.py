@@ -33,7 +33,6 @@ _IP = ctypes.POINTER(ctypes.c_int)
 _DP = ctypes.POINTER(ctypes.c_double)
 
 
-
 class MfbJob(ctypes.Structure):
     """struct mfb_job of include/mfb.h (field order and types as declared)."""
     _fields_ = [
@@ -94,8 +93,9 @@ SIGNATURES = {
     "mfb_hier_config": (_I, [_P, _SZP, _IP]),
     "mfb_hier_coarse_values": (_I, [_P, _I, _I, _I, _I, _SZ, _SZ, _P]),
     "mfb_fp32_peak": (_I, [_I, _DP]),
+    "mfb_hier_run_series": (_I, [_P, _P, _SZ, _P, _P, _P, _I, _I, _I, _SZ, _F, _P, _P, _P]),
     "mfb_adjoint": (_I, [_I, _SZ, _P, _I, _P, _I, _SZ, _P, _P, _P, _P, _P]),
-    "mfb_run_large_static":(_I, [_I, _SZ, _P, _I, _P, _I, _SZ, _F, _SZ, _SZ, _P, _P, _P, _P]),
+    "mfb_run_large_static": (_I, [_I, _SZ, _P, _I, _P, _I, _SZ, _F, _SZ, _SZ, _P, _P, _P, _P]),
 }
 
 _LIB = None

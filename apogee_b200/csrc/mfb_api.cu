@@ -1680,3 +1680,52 @@ extern "C" int mfb_batch_info(mfb_batch *b, int64_t *tickets, int *grid, int *se
   if (scratch_bytes) *scratch_bytes = b->scratch_bytes;
   return MFB_OK;
 }
+
+// ------------------------------------------------- hierarchical run_series
+extern "C" int mfb_hier_run_series(mfb_hplan *h, const void *series, size_t nseries,
+                                   const uint64_t *starts, const uint64_t *win_start,
+                                   const uint64_t *win_end, int nblocks, int t0, int nt,
+                                   size_t binsize, float threshold, int64_t *idx, void *val,
+                                   int32_t *counts) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  mfb_plan *p = h->full;
+  if (!series || !starts || !win_start || !win_end || nblocks < 1 || !idx || !val)
+    return fail(MFB_ERR_ARG, "invalid run_series arguments");
+  if (t0 < 0 || nt < 1 || t0 > p->nt - nt || binsize < 1)
+    return fail(MFB_ERR_ARG, "invalid template range or binsize");
+  size_t nb0 = 0;
+  for (int b = 0; b < nblocks; b++) {   // equal bin counts (src/hmf.c:199-213)
+    size_t lo = win_start[b], hi = win_end[b] > p->n ? p->n : win_end[b];
+    if (lo >= hi || starts[b] > (uint64_t)INT64_MAX - p->n)
+      return fail(MFB_ERR_ARG, "block %d has an empty window or an overflowing start", b);
+    size_t nb = 1 + (hi - lo - 1) / binsize;
+    if (b == 0) nb0 = nb;
+    else if (nb != nb0) return fail(MFB_ERR_ARG, "block windows must have equal bin counts");
+  }
+  DeviceGuard dg(h->device);
+  if (p->starts_cap < nblocks) {
+    cudaFree(p->starts_dev);
+    p->starts_dev = nullptr;
+    p->starts_cap = 0;
+    CUDA_TRY(cudaMalloc(&p->starts_dev, (size_t)nblocks * sizeof(uint64_t)));
+    p->starts_cap = nblocks;
+  }
+  CUDA_TRY(cudaMemcpyAsync(p->starts_dev, starts, (size_t)nblocks * sizeof(uint64_t),
+                           cudaMemcpyHostToDevice, p->stream));
+  // Runs of equal windows, at most ndata blocks each, transformed straight into
+  // the plan's data rows (src/hmf.c:171-197) and filtered hierarchically.
+  for (int b0 = 0; b0 < nblocks;) {
+    int g = 1;
+    while (g < p->nd && b0 + g < nblocks && win_start[b0 + g] == win_start[b0] &&
+           win_end[b0 + g] == win_end[b0])
+      g++;
+    int r = mfb_forward(p, series, nseries, p->starts_dev + b0, g, p->data);
+    if (r) return r;
+    r = hier_run_impl(h, 0, g, t0, nt, binsize, threshold, win_start[b0], win_end[b0],
+                      idx + (size_t)b0 * nt * nb0, (float2 *)val + (size_t)b0 * nt * nb0,
+                      counts ? counts + (size_t)b0 * nt : nullptr, 1);
+    if (r) return r;
+    b0 += g;
+  }
+  return MFB_OK;
+}

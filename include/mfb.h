@@ -140,6 +140,15 @@ int mfb_hier_run_phase(mfb_hplan *p, int phase, int d0, int nd, int t0, int nt, 
                        int32_t *counts);
 /* Survivors of the last mfb_hier_run (synchronises the plan's stream). */
 int mfb_hier_last_triggers(mfb_hplan *p, int64_t *triggers);
+/* Replaces ap_hmf_run_series (src/hmf.c:158-220): runs of blocks with equal
+   windows, at most ndata at a time, are forward-transformed on the device
+   into the plan's data rows (FFT(block/n), zero past nseries) and run through
+   mfb_hier_run.  Arguments and output as mfb_run_series; the plan's data rows
+   are scratch afterwards. */
+int mfb_hier_run_series(mfb_hplan *p, const void *series, size_t nseries, const uint64_t *starts,
+                        const uint64_t *win_start, const uint64_t *win_end, int nblocks,
+                        int t0, int nt, size_t binsize, float threshold,
+                        int64_t *idx, void *val, int32_t *counts);
 /* Replaces ap_hmf_stats (src/hmf.c:84-103): pairs and triggers since creation
    (synchronises the plan's stream).  Triggers are summed on the device, so
    runs need no host round trip and can be captured in a CUDA graph. */
