@@ -598,7 +598,8 @@ class HierarchicalFilter(MatchedFilter):
                 "gate model can place the threshold")
         for band in (self.n // 8, self.n // 4, self.n // 2):
             if band >= 64 and gatemodel.gate_for(self._pending_ref, self.n, band,
-                                                 self._fs_snr or self.snr, self.fd) is not None:
+                                                 self._fs_snr or self.snr, self.fd,
+                                                 device=self.device.index) is not None:
                 return band
         raise ValueError("the gate model cannot resolve fd=%g at snr=%g for n=%d"
                          % (self.fd, self.snr, self.n))
@@ -613,7 +614,9 @@ class HierarchicalFilter(MatchedFilter):
         key = (band, self._fs_snr or self.snr, self.fd, self._pending_ref.tobytes())
         if self._gate_cache is not None and self._gate_cache[0] == key:
             return self._gate_cache[1]
-        v = gatemodel.gate_for(self._pending_ref, self.n, band, self._fs_snr or self.snr, self.fd)
+        # the model's FP64 covariance work and its draws run on this device
+        v = gatemodel.gate_for(self._pending_ref, self.n, band, self._fs_snr or self.snr, self.fd,
+                               device=self.device.index)
         if v is None:
             raise ValueError("no calibrated coarse threshold for n=%d band=%d" % (self.n, band))
         if not np.isfinite(v) or v < 0 or v > float(np.finfo(np.float32).max):

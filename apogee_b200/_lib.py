@@ -94,6 +94,7 @@ SIGNATURES = {
     "mfb_hier_coarse_values": (_I, [_P, _I, _I, _I, _I, _SZ, _SZ, _P]),
     "mfb_fp32_peak": (_I, [_I, _DP]),
     "mfb_hier_run_series": (_I, [_P, _P, _SZ, _P, _P, _P, _I, _I, _I, _SZ, _F, _P, _P, _P]),
+    "mfb_gate_maxima": (_I, [_I, _P, _SZ, _SZ, _F, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _DP]),
     "mfb_adjoint": (_I, [_I, _SZ, _P, _I, _P, _I, _SZ, _P, _P, _P, _P, _P]),
     "mfb_run_large_static": (_I, [_I, _SZ, _P, _I, _P, _I, _SZ, _F, _SZ, _SZ, _P, _P, _P, _P]),
 }

@@ -25,6 +25,7 @@
 #include "large_kernel.cuh"
 #include "adjoint_kernel.cuh"
 #include "batch_kernel.cuh"
+#include "gate_kernels.cuh"
 
 using namespace mfb;
 
@@ -1727,5 +1728,90 @@ extern "C" int mfb_hier_run_series(mfb_hplan *h, const void *series, size_t nser
     if (r) return r;
     b0 += g;
   }
+  return MFB_OK;
+}
+
+// --------------------------------------------------------- gate model (device)
+extern "C" int mfb_gate_maxima(int device, const double *power, size_t n, size_t band, float snr,
+                               int step, int per, int has_out, const int32_t *taus,
+                               const int32_t *ntaus, const int32_t *on_grid, const void *draw_in,
+                               const void *draw_out, float *coarse, float *fine,
+                               double *sums_out) {
+  if (!power || !taus || !ntaus || !on_grid || !draw_in || !coarse || !fine)
+    return fail(MFB_ERR_ARG, "gate model: null pointer");
+  if (n < 64 || n > ((size_t)1 << 20) || band < 1 || band > n || n % band)
+    return fail(MFB_ERR_ARG, "gate model: band must divide n (n <= 2^20)");
+  if (step != (int)(n / band) || per < 1 || (has_out && !draw_out))
+    return fail(MFB_ERR_ARG, "gate model: bad step, per or out-of-band draws");
+  if (!std::isfinite(snr) || snr <= 0.f) return fail(MFB_ERR_ARG, "gate model: bad snr");
+  const int dmax = 8 * step + 8;
+  for (int o = 0; o < step; o++) {
+    const int K = ntaus[o];
+    if (K < 1 || K > GATE_K) return fail(MFB_ERR_ARG, "gate model: %d lags at offset %d", K, o);
+    for (int i = 0; i < K; i++) {
+      const int t = taus[o * GATE_K + i];
+      if (t < -dmax / 2 || t > dmax / 2 || t - o < -dmax || t - o > dmax)
+        return fail(MFB_ERR_ARG, "gate model: lag %d outside the table", t);
+    }
+    for (int g = 0; g < GATE_GRID; g++)
+      if (on_grid[o * GATE_GRID + g] < 0 || on_grid[o * GATE_GRID + g] >= K)
+        return fail(MFB_ERR_ARG, "gate model: grid index out of range");
+  }
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(MFB_ERR_ARG, "no device %d", device);
+  DeviceGuard dg(device);
+  const size_t nl = 2 * (size_t)dmax + 1, kk = (size_t)GATE_K * GATE_K;
+  const size_t draws = (size_t)step * per * GATE_K * sizeof(float2);
+  const size_t bytes[] = {n * sizeof(double), 2 * sizeof(double), nl * sizeof(double2),
+                          nl * sizeof(double2), (size_t)step * GATE_K * sizeof(int),
+                          (size_t)step * sizeof(int), (size_t)step * GATE_GRID * sizeof(int),
+                          step * kk * sizeof(float2), step * kk * sizeof(float2),
+                          (size_t)step * GATE_K * sizeof(float2), (size_t)step * GATE_K * sizeof(float2),
+                          draws, has_out ? draws : 0, (size_t)step * per * sizeof(float),
+                          (size_t)step * per * sizeof(float)};
+  constexpr int NB = sizeof(bytes) / sizeof(bytes[0]);
+  size_t off[NB + 1];
+  off[0] = 0;
+  for (int i = 0; i < NB; i++) off[i + 1] = off[i] + ((bytes[i] + 255) & ~(size_t)255);
+  char *mem = nullptr;
+  CUDA_TRY(cudaMalloc(&mem, off[NB]));
+  std::unique_ptr<char, cudaError_t (*)(void *)> guard(mem, cudaFree);
+  GateArgs a;
+  memset(&a, 0, sizeof a);
+  a.power = (const double *)(mem + off[0]);
+  a.sums = (double *)(mem + off[1]);
+  a.a_full = (double2 *)(mem + off[2]);
+  a.a_band = (double2 *)(mem + off[3]);
+  a.taus = (const int *)(mem + off[4]);
+  a.ntaus = (const int *)(mem + off[5]);
+  a.on_grid = (const int *)(mem + off[6]);
+  a.l_in = (float2 *)(mem + off[7]);
+  a.l_out = (float2 *)(mem + off[8]);
+  a.s_full = (float2 *)(mem + off[9]);
+  a.s_band = (float2 *)(mem + off[10]);
+  a.draw_in = (const float2 *)(mem + off[11]);
+  a.draw_out = has_out ? (const float2 *)(mem + off[12]) : nullptr;
+  a.coarse = (float *)(mem + off[13]);
+  a.fine = (float *)(mem + off[14]);
+  a.n = (int)n; a.band = (int)band; a.dmax = dmax;
+  a.step = step; a.per = per; a.has_out = has_out; a.snr = snr;
+  CUDA_TRY(cudaMemcpy(mem + off[0], power, bytes[0], cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(mem + off[4], taus, bytes[4], cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(mem + off[5], ntaus, bytes[5], cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(mem + off[6], on_grid, bytes[6], cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(mem + off[11], draw_in, draws, cudaMemcpyHostToDevice));
+  if (has_out) CUDA_TRY(cudaMemcpy(mem + off[12], draw_out, draws, cudaMemcpyHostToDevice));
+  gate_sums_kernel<<<1, 1024>>>(a);
+  CUDA_TRY(cudaGetLastError());
+  gate_lags_kernel<<<(unsigned)nl, 256>>>(a);
+  CUDA_TRY(cudaGetLastError());
+  gate_chol_kernel<<<(step + 63) / 64, 64>>>(a);
+  CUDA_TRY(cudaGetLastError());
+  gate_draw_kernel<<<dim3((unsigned)((per + 127) / 128), (unsigned)step), 128>>>(a);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpy(coarse, a.coarse, bytes[13], cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(fine, a.fine, bytes[14], cudaMemcpyDeviceToHost));
+  if (sums_out) CUDA_TRY(cudaMemcpy(sums_out, a.sums, 2 * sizeof(double), cudaMemcpyDeviceToHost));
   return MFB_OK;
 }

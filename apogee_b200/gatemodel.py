@@ -1,4 +1,4 @@
-"""Coarse-gate threshold from the reference power profile (host, numpy).
+"""Coarse-gate threshold from the reference power profile.
 
 Restates the reference's Monte-Carlo gate model
 (python/matchedfilter/gatemodel.py:63-227), which has to stay alike because
@@ -13,6 +13,10 @@ draw complex Gaussian noise with those covariances (Cholesky in FP64,
 draws in FP32), form the coarse maximum over the coarse grid lags and the
 fine maximum over nearby integer lags, keep the coarse maxima of draws
 whose fine maximum reaches snr, and return their fd-quantile.
+
+gate_for(..., device=k) runs the numerics on GPU k (FP64 sums, covariances
+and Cholesky factors, FP32 transforms and maxima; gate_kernels.cuh) with the
+same draws; without `device` they run here in numpy.
 
 Noise convention: Re and Im of the output each have variance 1, so a
 complex draw normalised to E|z|^2 = 1 is scaled by sqrt(2)
@@ -89,17 +93,71 @@ def joint_maxima(power, n, band, snr, nsamp, seed=SEED):
     return np.concatenate(coarse), np.concatenate(fine)
 
 
-def kept_coarse(power, n, band, snr, nsamp, seed=SEED):
-    """Sorted coarse maxima of the draws the fine stage keeps (cached)."""
+GRID_POINTS = 2 * COARSE_LAGS + 1
+MAX_TAUS = 16
+
+
+def joint_maxima_device(power, n, band, snr, nsamp, seed=SEED, device=0):
+    """joint_maxima with its numerics on the GPU (mfb_gate_maxima): FP64
+    profile sums, lag covariances and Cholesky factors, FP32 noise transforms
+    and maxima.  The draws are the same seeded numpy stream, drawn here in the
+    same order, so the estimator is the host one draw for draw."""
+    import ctypes
+    from . import _lib
+    q = np.asarray(power, dtype=np.float64)
+    total = q.sum()
+    if total <= 0:
+        return None
+    q = q / total
+    f = min(max(float(q[:band].sum()), 0.0), 1.0)
+    if f == 0:
+        return None
+    step = n // band
+    has_out = (1.0 - f) > 1e-9
+    grid = np.arange(-COARSE_LAGS, COARSE_LAGS + 1) * step
+    rng = np.random.default_rng(seed)
+    per = max(nsamp // step, 256)
+    taus_all = np.zeros((step, MAX_TAUS), np.int32)
+    ntaus = np.zeros(step, np.int32)
+    on_grid = np.zeros((step, GRID_POINTS), np.int32)
+    d_in = np.zeros((step, per, MAX_TAUS), np.complex64)
+    d_out = np.zeros((step, per, MAX_TAUS), np.complex64) if has_out else None
+    for off in range(step):
+        taus = np.unique(np.concatenate([np.arange(-FINE_LAGS, FINE_LAGS + 1) + off, grid]))
+        k = len(taus)
+        taus_all[off, :k] = taus
+        ntaus[off] = k
+        on_grid[off] = np.searchsorted(taus, grid)
+        d_in[off, :, :k] = _draw(rng, per, k)
+        if has_out:
+            d_out[off, :, :k] = _draw(rng, per, k)
+    coarse = np.empty(step * per, np.float32)
+    fine = np.empty(step * per, np.float32)
+    sums = np.empty(2, np.float64)
+    q64 = np.ascontiguousarray(q, dtype=np.float64)
+    _lib.check(_lib.lib().mfb_gate_maxima(
+        int(device), q64.ctypes.data, n, band, float(snr), step, per, int(has_out),
+        taus_all.ctypes.data, ntaus.ctypes.data, on_grid.ctypes.data, d_in.ctypes.data,
+        None if d_out is None else d_out.ctypes.data, coarse.ctypes.data, fine.ctypes.data,
+        sums.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "gate model failed")
+    return coarse, fine
+
+
+def kept_coarse(power, n, band, snr, nsamp, seed=SEED, device=None):
+    """Sorted coarse maxima of the draws the fine stage keeps (cached);
+    `device` (a CUDA ordinal) runs the numerics there."""
     p = np.asarray(power, dtype=np.float64)
     if (p.shape != (n,) or not np.isfinite(p).all() or (p < 0).any() or p.sum() <= 0):
         raise ValueError("power must be a finite nonnegative length-n profile with positive sum")
     p = p / p.sum()
-    key = (p.tobytes(), n, band, float(snr), nsamp, seed)
+    key = (p.tobytes(), n, band, float(snr), nsamp, seed, device)
     if key in _cache:
         _cache.move_to_end(key)
         return _cache[key]
-    got = joint_maxima(p, n, band, snr, nsamp, seed)
+    if device is None:
+        got = joint_maxima(p, n, band, snr, nsamp, seed)
+    else:
+        got = joint_maxima_device(p, n, band, snr, nsamp, seed, device)
     if got is None:
         return None
     c, fmax = got
@@ -126,14 +184,15 @@ def _validate(n, band, snr, fd):
         raise ValueError("fd must be finite and between zero and one")
 
 
-def gate_for(power, n, band, snr, fd):
+def gate_for(power, n, band, snr, fd, device=None):
     """Largest coarse threshold whose modelled dismissal meets fd, or None
-    when the draws cannot resolve the budget."""
+    when the draws cannot resolve the budget.  With `device` (a CUDA ordinal)
+    the FP64 covariance work and the FP32 draws run on that GPU."""
     _validate(n, band, snr, fd)
     nsamp = samples_for(fd)
     if fd * nsamp < 8:
         return None
-    kept = kept_coarse(power, n, band, snr, nsamp)
+    kept = kept_coarse(power, n, band, snr, nsamp, device=device)
     if kept is None or not len(kept):
         return None
     i = int(np.floor(float(fd) * len(kept)))

@@ -265,6 +265,23 @@ int mfb_run_large_static(int device, size_t n, const void *data, int nd, const v
                          int nt, size_t binsize, float threshold, size_t start, size_t end,
                          int64_t *idx, void *val, int32_t *counts, void *stream);
 
+/* ---- coarse-gate model ------------------------------------------------------ */
+
+/* Replaces the numerics of the reference's gate model joint_maxima
+   (python/matchedfilter/gatemodel.py:63-140) on the device: FP64 profile sums,
+   lag covariances of the full and in-band profile and their Cholesky factors,
+   then the FP32 noise transforms and the coarse / fine maxima of every draw.
+   HOST arguments: power [n] (FP64); step = n/band sub-grid offsets; taus [step][16]
+   (the offset's lags, ntaus[step] of them, ascending); on_grid [step][9] (the
+   coarse grid lags' positions in taus); draw_in / draw_out complex64
+   [step][per][16] (the model's standard normal draws / sqrt 2, zero past
+   ntaus; draw_out ignored unless has_out).  Outputs HOST coarse, fine
+   [step][per] and sums_out[2] = (sum power, sum of the lowest band bins). */
+int mfb_gate_maxima(int device, const double *power, size_t n, size_t band, float snr, int step,
+                    int per, int has_out, const int32_t *taus, const int32_t *ntaus,
+                    const int32_t *on_grid, const void *draw_in, const void *draw_out,
+                    float *coarse, float *fine, double *sums_out);
+
 /* ---- measurement --------------------------------------------------------- */
 
 /* Measured FP32 FMA throughput of `device` in FLOP/s (2 per FMA), from a
