@@ -18,15 +18,17 @@
 // along M: stage 1 rows are (pair, f2) -- 4 pairs per 128-row tile -- and
 // stage 2 rows are (pair, j1) -- 8 pairs per tile.
 //
-// Per CTA iteration (8 pairs): the conjugate product and its split are
-// written by the CUDA cores as the stage-1 A operand (K-major, no swizzle);
-// one thread issues 12 MMAs (M128 N32 K16) into TMEM; the accumulators come
-// back with tcgen05.ld, are twiddled, split and written transposed as the
-// stage-2 A operand (K-major, 128-byte swizzle, so a warp's 32 stores to one
-// row hit 32 different banks); 12 more MMAs (M128 N64 K16); then |z|^2 over
-// the window, max over the pair's 16 rows, and the gate of src/hmf.c:264-300.
-// The DFT matrices (B operands) and the 512-point twiddles are built once on
-// the host in FP64 and copied into shared memory at kernel start.
+// Per item (8 pairs): the conjugate product and its split are written by the
+// CUDA cores as the stage-1 A operand (K-major, no swizzle); one thread
+// issues 12 MMAs (M128 N32 K16) into TMEM; the accumulators come back with
+// tcgen05.ld, are twiddled, split and written transposed as the stage-2 A
+// operand (K-major, 128-byte swizzle, so a warp's 32 stores to one row hit 32
+// different banks); 12 more MMAs (M128 N64 K16); then |z|^2 over the window,
+// max over the pair's 16 rows, and the gate of src/hmf.c:264-300.  The three
+// steps run in separate warp roles on consecutive items (see
+// coarse_tc_ws_kernel).  The DFT matrices (B operands) and the 512-point
+// twiddles are built once on the host in FP64 and copied into shared memory
+// at kernel start.
 //
 // Every wait on an mbarrier is bounded; on timeout the kernel records an
 // error flag, stops issuing work, releases its tensor memory and returns.
@@ -42,19 +44,12 @@ namespace mfb {
 
 namespace tc {
 constexpr int BAND = 512;
-constexpr int PAIRS = 8;          // pairs per CTA iteration; warp w works on pair w
-constexpr int THREADS = 256;
-constexpr int TMEM_COLS = 128;    // stage 1: 2 x 32 columns, stage 2: 64 columns
-// shared-memory layout, offsets from a 1024-byte aligned base
+constexpr int PAIRS = 8;          // pairs per item; producer warp w works on pair w
+// constant operands at the start of shared memory (1024-byte aligned base)
 constexpr int OFF_B2 = 0;         // 2 splits x 8 KB, 128B swizzle (64 rows x 128 B)
 constexpr int OFF_B1 = 16384;     // 2 splits x 2 k-steps x 1 KB, no swizzle
 constexpr int OFF_TW = 20480;     // 512 float2 twiddles W512^(f2 j1), [j1][f2]
 constexpr int CONST_BYTES = 24576;
-constexpr int OFF_A2 = 24576;     // 2 splits x 16 KB, 128B swizzle (128 rows x 128 B)
-constexpr int OFF_A1 = 57344;     // 2 tiles x 2 splits x 2 k-steps x 4 KB, no swizzle
-constexpr int OFF_BEST = 90112;   // 2 x 128 floats: per-row partial maxima of stage 2
-constexpr int OFF_BAR = 91136;    // 2 mbarriers (8 B each) + TMEM address slot
-constexpr int SMEM_BYTES = OFF_BAR + 64 + 1024;   // + alignment slack
 constexpr unsigned SPIN_LIMIT = 1u << 22;
 
 __host__ __device__ constexpr uint32_t idesc(int n, int fp16) {
@@ -160,30 +155,84 @@ struct TcKernelArgs {
   int *err;
 };
 
+// Warp-specialised form of the same pass: three roles in one 512-thread CTA
+// (one per SM) work on consecutive items at once, handing operands over
+// through NSLOT shared-memory and tensor-memory slots per stage:
+//   warps 0-7   producers: warp w owns pair w of the item (lane = f2); the
+//               conjugate product and split -> stage-1 A (slot k), inputs for
+//               the next item already in flight; thread 0 issues the stage-1
+//               MMAs into TMEM S1[k];
+//   warps 8-11  stage-1 epilogue: quadrant q reads pairs q and 4 + q from
+//               S1[k] -> twiddle, split, transposed store -> stage-2 A
+//               (slot k); thread 256 issues the stage-2 MMAs into S2[k];
+//   warps 12-15 stage-2 epilogue: S2[k] -> |z|^2 over the window, max per
+//               pair with warp shuffles, gate.
+// Hand-offs are mbarriers: full_s1[k] / full_s2[k] (MMA commits) and
+// free_s1[k] / free_s2[k] (the epilogue warps have read the accumulators).
+// A slot is reused every NSLOT items, so each wait is on the phase of the
+// item NSLOT back and no role can run two phases ahead of a waiter.  Waits
+// are bounded; a failed wait sets the error flag, every later wait returns
+// at once and the roles run out their loops without issuing MMAs (no thread
+// leaves a loop early, so the role barriers always fill).
+namespace tcw {
+constexpr int NSLOT = 2;
+constexpr int THREADS = 512;
+constexpr int TMEM_COLS = 256;                      // S1[2] x 64 + S2[2] x 64
+constexpr int S2_COL = NSLOT * 64;
+constexpr int SLOT = 32768;
+constexpr int OFF_A2 = 24576;                       // NSLOT x 32 KB (2 splits x 16 KB, 128B swizzle)
+constexpr int OFF_A1 = OFF_A2 + NSLOT * SLOT;       // NSLOT x 32 KB (2 tiles x 2 splits x 2 k-steps x 4 KB)
+constexpr int OFF_BAR = OFF_A1 + NSLOT * SLOT;      // 4 NSLOT mbarriers, TMEM slot, abort flag
+constexpr int SMEM_BYTES = OFF_BAR + 128 + 1024;
+constexpr int B_FULL1 = 0, B_FULL2 = NSLOT, B_FREE1 = 2 * NSLOT, B_FREE2 = 3 * NSLOT;
+}  // namespace tcw
+
+__device__ __forceinline__ void role_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(nthreads) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(bar) : "memory");
+}
+// Bounded wait that gives up at once when another thread has given up.
+__device__ __forceinline__ bool mbar_wait_ab(uint32_t bar, uint32_t phase, volatile int *abort_flag,
+                                             int *err) {
+  for (unsigned i = 0; i < tc::SPIN_LIMIT; i++) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}\n" : "=r"(ok) : "r"(bar), "r"(phase) : "memory");
+    if (ok) return true;
+    if (*abort_flag) return false;
+  }
+  *err = 1;
+  *abort_flag = 1;
+  return false;
+}
+
 template <int FP16>
-__global__ void __launch_bounds__(tc::THREADS, 2)
-coarse_tc_kernel(const TcKernelArgs a) {
+__global__ void __launch_bounds__(tcw::THREADS, 1)
+coarse_tc_ws_kernel(const TcKernelArgs a) {
   using namespace tc;
+  using tcw::NSLOT;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *sm = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t sbase = smem_u32(sm);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(sm + OFF_BAR);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + OFF_BAR + 16);
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(sm + OFF_BAR + 24);
-
-  // constants (B operands, twiddles) into shared memory
-  for (int i = tid; i < CONST_BYTES / 16; i += THREADS)
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sm + tcw::OFF_BAR);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + tcw::OFF_BAR + 8 * 4 * NSLOT);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(sm + tcw::OFF_BAR + 8 * 4 * NSLOT + 8);
+  for (int i = tid; i < CONST_BYTES / 16; i += tcw::THREADS)
     reinterpret_cast<uint4 *>(sm)[i] = a.consts[i];
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bars[0])));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bars[1])));
+    for (int i = 0; i < 4 * NSLOT; i++) {   // commits: 1 arrival; epilogue reads: 1 per warp (4)
+      const int cnt = i < tcw::B_FREE1 ? 1 : 4;
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&bars[i])), "r"(cnt));
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     *abort_flag = 0;
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                 :: "r"(smem_u32(tslot)), "r"(TMEM_COLS));
+                 :: "r"(smem_u32(tslot)), "r"(tcw::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   fence_async_smem();
@@ -193,191 +242,198 @@ coarse_tc_kernel(const TcKernelArgs a) {
   const uint32_t tmem = *tslot;
   const float2 *tw512 = reinterpret_cast<const float2 *>(sm + OFF_TW);
   const uint32_t id1 = idesc(32, FP16), id2 = idesc(64, FP16);
-  uint32_t phase0 = 0, phase1 = 0;
-
   const long long total = (long long)a.nd * a.nt;
   const long long items = (total + PAIRS - 1) / PAIRS;
   const long long per = items / gridDim.x, extra = items % gridDim.x;
   const long long ibeg = blockIdx.x * per + (blockIdx.x < extra ? blockIdx.x : extra);
-  const long long iend = ibeg + per + (blockIdx.x < extra ? 1 : 0);
+  const int nit = (int)(per + (blockIdx.x < extra ? 1 : 0));
+  auto bar = [&](int i) { return smem_u32(&bars[i]); };
 
-  // Software pipeline over items (8 pairs each), per iteration i:
-  //   wait stage 1 (i); stage-1 epilogue (i) -> A2; issue stage 2 (i)
-  //   product (i+1) -> A1 from loads issued before the epilogue; issue stage 1 (i+1)
-  //   wait stage 2 (i); gate (i)
-  // so stage 2 (i) overlaps the product of i+1 and stage 1 (i+1) overlaps the
-  // gate of i.  Each thread owns one stage-1 row: pair = warp, f2 = lane.
-  const int prow = tid & 127, ptile = warp >> 2;
-  float2 pd[16], ph[16];
-  auto issue_loads = [&](long long item) {
-    const long long pi = item * PAIRS + warp;
-    if (item < iend && pi < total) {
-      const int d = (int)(pi / a.nt), t = (int)(pi - (long long)d * a.nt);
-      const float2 *dp = a.data + (long long)(a.d0 + d) * a.data_stride;
-      const float2 *hp = a.ct + (long long)(a.t0 + t) * BAND;
+  if (warp < 8) {
+    // ---- producers: warp w owns pair w of the item, lane = f2 ----------------
+    const int prow = 32 * (warp & 3) + lane, ptile = warp >> 2;
+    float2 pd[16], ph[16];
+    auto issue_loads = [&](int it) {
+      const long long pi = (ibeg + it) * PAIRS + warp;
+      if (it < nit && pi < total) {
+        const int d = (int)(pi / a.nt), t = (int)(pi - (long long)d * a.nt);
+        const float2 *dp = a.data + (long long)(a.d0 + d) * a.data_stride;
+        const float2 *hp = a.ct + (long long)(a.t0 + t) * BAND;
 #pragma unroll
-      for (int f1 = 0; f1 < 16; f1++) { pd[f1] = __ldg(dp + 32 * f1 + lane); ph[f1] = __ldg(hp + 32 * f1 + lane); }
-    } else {
+        for (int f1 = 0; f1 < 16; f1++) { pd[f1] = __ldg(dp + 32 * f1 + lane); ph[f1] = __ldg(hp + 32 * f1 + lane); }
+      } else {
 #pragma unroll
-      for (int f1 = 0; f1 < 16; f1++) { pd[f1] = make_float2(0.f, 0.f); ph[f1] = make_float2(0.f, 0.f); }
-    }
-  };
-  auto produce = [&]() {
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      uint32_t hh[4], ll[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const float2 x = pd[4 * q + u], h = ph[4 * q + u];
-        split2<FP16>(fmaf(x.x, h.x, x.y * h.y), fmaf(x.y, h.x, -x.x * h.y), hh[u], ll[u]);
+        for (int f1 = 0; f1 < 16; f1++) { pd[f1] = make_float2(0.f, 0.f); ph[f1] = make_float2(0.f, 0.f); }
       }
-      const int ks = q >> 1, cc = q & 1;
-      const int off = (prow >> 3) * 256 + cc * 128 + (prow & 7) * 16;
-      *reinterpret_cast<uint4 *>(sm + OFF_A1 + ((ptile * 2 + 0) * 2 + ks) * 4096 + off) =
-          make_uint4(hh[0], hh[1], hh[2], hh[3]);
-      *reinterpret_cast<uint4 *>(sm + OFF_A1 + ((ptile * 2 + 1) * 2 + ks) * 4096 + off) =
-          make_uint4(ll[0], ll[1], ll[2], ll[3]);
+    };
+    int last = -1;
+    issue_loads(0);
+    for (int it = 0; it < nit; it++) {
+      const int k = it % NSLOT;
+      const uint32_t u = (uint32_t)(it / NSLOT);
+      if (it >= NSLOT) mbar_wait_ab(bar(tcw::B_FULL1 + k), (u - 1) & 1, abort_flag, a.err);  // A1[k] consumed
+      uint8_t *a1 = sm + tcw::OFF_A1 + k * tcw::SLOT;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        uint32_t hh[4], ll[4];
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          const float2 x = pd[4 * q + v], h = ph[4 * q + v];
+          split2<FP16>(fmaf(x.x, h.x, x.y * h.y), fmaf(x.y, h.x, -x.x * h.y), hh[v], ll[v]);
+        }
+        const int ks = q >> 1, cc = q & 1;
+        const int off = (prow >> 3) * 256 + cc * 128 + (prow & 7) * 16;
+        *reinterpret_cast<uint4 *>(a1 + ((ptile * 2 + 0) * 2 + ks) * 4096 + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+        *reinterpret_cast<uint4 *>(a1 + ((ptile * 2 + 1) * 2 + ks) * 4096 + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+      }
+      issue_loads(it + 1);
+      fence_async_smem();
+      tc_before_sync();
+      role_sync(1, 256);
+      if (tid == 0) {
+        bool ok = !*abort_flag;
+        if (ok && it >= NSLOT)
+          ok = mbar_wait_ab(bar(tcw::B_FREE1 + k), (u - 1) & 1, abort_flag, a.err);   // S1[k] read
+        if (ok) {
+          tc_after_sync();
+          const uint32_t a1s = sbase + tcw::OFF_A1 + k * tcw::SLOT;
+#pragma unroll
+          for (int s = 0; s < 2; s++) {
+            int first = 1;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+              const int ha = (c == 2) ? 1 : 0, hb = (c == 1) ? 1 : 0;
+#pragma unroll
+              for (int ks = 0; ks < 2; ks++) {
+                const uint64_t ad = sdesc(a1s + ((s * 2 + ha) * 2 + ks) * 4096, 128, 256, 0);
+                const uint64_t bd = sdesc(sbase + OFF_B1 + (hb * 2 + ks) * 1024, 128, 256, 0);
+                mma(tmem + k * 64 + s * 32, ad, bd, id1, first ? 0u : 1u);
+                first = 0;
+              }
+            }
+          }
+          commit(bar(tcw::B_FULL1 + k));
+          last = it;
+        }
+      }
     }
-  };
-  auto issue_stage1 = [&]() {
-    if (tid == 0) {
+    if (tid == 0 && last >= 0)   // own MMAs complete before the accumulators are freed
+      mbar_wait(bar(tcw::B_FULL1 + last % NSLOT), (uint32_t)(last / NSLOT) & 1);
+  } else if (warp < 12) {
+    // ---- stage-1 epilogue: quadrant q, pairs q (tile 0) and 4 + q (tile 1), f2 = lane
+    const int q = warp & 3, f2 = lane;
+    int last = -1;
+    for (int it = 0; it < nit; it++) {
+      const int k = it % NSLOT;
+      const uint32_t u = (uint32_t)(it / NSLOT);
+      mbar_wait_ab(bar(tcw::B_FULL1 + k), u & 1, abort_flag, a.err);                       // S1[k] full
+      tc_after_sync();
+      uint32_t v0[32], v1[32];
+      MFB_TMEM_LD32(tmem + ((uint32_t)(32 * q) << 16) + k * 64, v0);
+      MFB_TMEM_LD32(tmem + ((uint32_t)(32 * q) << 16) + k * 64 + 32, v1);
+      tmem_wait_ld();
+      tc_before_sync();
+      if (lane == 0) mbar_arrive(bar(tcw::B_FREE1 + k));
+      if (it >= NSLOT) mbar_wait_ab(bar(tcw::B_FULL2 + k), (u - 1) & 1, abort_flag, a.err);  // A2[k] consumed
+      uint8_t *a2 = sm + tcw::OFF_A2 + k * tcw::SLOT;
 #pragma unroll
       for (int s = 0; s < 2; s++) {
-        int first = 1;
+        const int p = 4 * s + q;
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-          const int ha = (c == 2) ? 1 : 0, hb = (c == 1) ? 1 : 0;
+        for (int j1 = 0; j1 < 16; j1++) {
+          const uint32_t *vv = s ? v1 : v0;
+          const float yr = __uint_as_float(vv[2 * j1]), yi = __uint_as_float(vv[2 * j1 + 1]);
+          const float2 w = tw512[j1 * 32 + f2];
+          const float zr = fmaf(yr, w.x, -yi * w.y), zi = fmaf(yr, w.y, yi * w.x);
+          uint32_t hi, lo;
+          split2<FP16>(zr, zi, hi, lo);
+          const int R = p * 16 + j1;
+          const int off = (R >> 3) * 1024 + (R & 7) * 128 + (((f2 >> 2) ^ (R & 7)) << 4) + (f2 & 3) * 4;
+          *reinterpret_cast<uint32_t *>(a2 + off) = hi;
+          *reinterpret_cast<uint32_t *>(a2 + 16384 + off) = lo;
+        }
+      }
+      fence_async_smem();
+      tc_before_sync();
+      role_sync(2, 128);
+      if (tid == 256) {
+        bool ok = !*abort_flag;
+        if (ok && it >= NSLOT)
+          ok = mbar_wait_ab(bar(tcw::B_FREE2 + k), (u - 1) & 1, abort_flag, a.err);   // S2[k] read
+        if (ok) {
+          tc_after_sync();
+          const uint32_t a2s = sbase + tcw::OFF_A2 + k * tcw::SLOT;
+          int first = 1;
 #pragma unroll
-          for (int ks = 0; ks < 2; ks++) {
-            const uint64_t ad = sdesc(sbase + OFF_A1 + ((s * 2 + ha) * 2 + ks) * 4096, 128, 256, 0);
-            const uint64_t bd = sdesc(sbase + OFF_B1 + (hb * 2 + ks) * 1024, 128, 256, 0);
-            mma(tmem + s * 32, ad, bd, id1, first ? 0u : 1u);
-            first = 0;
+          for (int c = 0; c < 3; c++) {
+            const int ha = (c == 2) ? 1 : 0, hb = (c == 1) ? 1 : 0;
+#pragma unroll
+            for (int ks = 0; ks < 4; ks++) {
+              const uint64_t ad = sdesc(a2s + ha * 16384 + ks * 32, 16, 1024, 2);
+              const uint64_t bd = sdesc(sbase + OFF_B2 + hb * 8192 + ks * 32, 16, 1024, 2);
+              mma(tmem + tcw::S2_COL + k * 64, ad, bd, id2, first ? 0u : 1u);
+              first = 0;
+            }
           }
+          commit(bar(tcw::B_FULL2 + k));
+          last = it;
         }
       }
-      commit(smem_u32(&bars[0]));
     }
-  };
-  auto issue_stage2 = [&]() {
-    if (tid == 0) {
-      int first = 1;
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        const int ha = (c == 2) ? 1 : 0, hb = (c == 1) ? 1 : 0;
-#pragma unroll
-        for (int ks = 0; ks < 4; ks++) {
-          const uint64_t ad = sdesc(sbase + OFF_A2 + ha * 16384 + ks * 32, 16, 1024, 2);
-          const uint64_t bd = sdesc(sbase + OFF_B2 + hb * 8192 + ks * 32, 16, 1024, 2);
-          mma(tmem + 64, ad, bd, id2, first ? 0u : 1u);
-          first = 0;
-        }
-      }
-      commit(smem_u32(&bars[1]));
-    }
-  };
-  auto publish = [&]() {   // generic-proxy smem writes -> visible to the tensor cores
-    fence_async_smem();
-    tc_before_sync();
-    __syncthreads();
-    tc_after_sync();
-  };
-
-  if (ibeg < iend) {
-    issue_loads(ibeg);
-    produce();
-    publish();
-    issue_stage1();
-  }
-  for (long long item = ibeg; item < iend; ++item) {
-    issue_loads(item + 1);                       // consumed after the stage-1 epilogue
-    if (!mbar_wait(smem_u32(&bars[0]), phase0)) { *a.err = 1; *abort_flag = 1; }
-    phase0 ^= 1;
-    tc_after_sync();
-    // ---- stage-1 epilogue: twiddle, split, transpose -> stage-2 A (SW128) ---
-    {
-      const int s = warp >> 2, p = warp, f2 = lane;
-      uint32_t v[32];
-      MFB_TMEM_LD32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + s * 32, v);
-      tmem_wait_ld();
-#pragma unroll
-      for (int j1 = 0; j1 < 16; j1++) {
-        const float yr = __uint_as_float(v[2 * j1]), yi = __uint_as_float(v[2 * j1 + 1]);
-        const float2 w = tw512[j1 * 32 + f2];
-        const float zr = fmaf(yr, w.x, -yi * w.y), zi = fmaf(yr, w.y, yi * w.x);
-        uint32_t hi, lo;
-        split2<FP16>(zr, zi, hi, lo);
-        const int R = p * 16 + j1;
-        const int off = (R >> 3) * 1024 + (R & 7) * 128 + (((f2 >> 2) ^ (R & 7)) << 4) + (f2 & 3) * 4;
-        *reinterpret_cast<uint32_t *>(sm + OFF_A2 + off) = hi;
-        *reinterpret_cast<uint32_t *>(sm + OFF_A2 + 16384 + off) = lo;
-      }
-    }
-    publish();
-    if (*abort_flag) break;
-    issue_stage2();
-    // ---- product of the next item while stage 2 runs -------------------------
-    const bool more = item + 1 < iend;
-    if (more) {
-      produce();
-      publish();
-      issue_stage1();
-    }
-    if (!mbar_wait(smem_u32(&bars[1]), phase1)) { *a.err = 1; *abort_flag = 1; }
-    phase1 ^= 1;
-    tc_after_sync();
-    // ---- stage-2 epilogue: |z|^2 over the window, max per pair, gate --------
-    // Warps 0-3 take columns j2 = 0..15, warps 4-7 j2 = 16..31 of rows
-    // R = 32 (w % 4) + lane = (pair R / 16, j1 = R % 16).
-    {
-      float *bestbuf = reinterpret_cast<float *>(sm + OFF_BEST);
-      uint32_t v[32];
-      const int half = warp >> 2, R = 32 * (warp & 3) + lane, j1 = R & 15;
-      MFB_TMEM_LD32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + 64 + 32 * half, v);
-      tmem_wait_ld();
+    if (tid == 256 && last >= 0)
+      mbar_wait(bar(tcw::B_FULL2 + last % NSLOT), (uint32_t)(last / NSLOT) & 1);
+  } else {
+    // ---- stage-2 epilogue: quadrant q, rows R = 32 q + lane = (pair R / 16, j1 = R % 16)
+    const int q = warp & 3, R = 32 * q + lane, j1 = R & 15;
+    for (int it = 0; it < nit; it++) {
+      const int k = it % NSLOT;
+      const uint32_t u = (uint32_t)(it / NSLOT);
+      mbar_wait_ab(bar(tcw::B_FULL2 + k), u & 1, abort_flag, a.err);                       // S2[k] full
+      tc_after_sync();
       float best = 0.f;
 #pragma unroll
-      for (int jj = 0; jj < 16; jj++) {
-        const float zr = __uint_as_float(v[2 * jj]), zi = __uint_as_float(v[2 * jj + 1]);
-        const int j = j1 + 16 * (16 * half + jj);
-        const float m2 = fmaf(zr, zr, zi * zi);
-        if (j >= a.ws && j < a.we && m2 > best) best = m2;
-      }
-      bestbuf[half * 128 + R] = best;
-      __syncthreads();
-      if (tid < 128) {
-        best = fmaxf(bestbuf[tid], bestbuf[128 + tid]);
+      for (int half = 0; half < 2; half++) {
+        uint32_t v[32];
+        MFB_TMEM_LD32(tmem + ((uint32_t)(32 * q) << 16) + tcw::S2_COL + k * 64 + 32 * half, v);
+        tmem_wait_ld();
 #pragma unroll
-        for (int o = 8; o; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
-        const int p = tid >> 4;
-        const long long pi = item * PAIRS + p;
-        if (pi < total) {
-          const int row = (int)pi;
-          if (a.coarse_out) {
-            if ((lane & 15) == 0) a.coarse_out[row] = sqrtf(best);
+        for (int jj = 0; jj < 16; jj++) {
+          const float zr = __uint_as_float(v[2 * jj]), zi = __uint_as_float(v[2 * jj + 1]);
+          const int j = j1 + 16 * (16 * half + jj);
+          const float m2 = fmaf(zr, zr, zi * zi);
+          if (j >= a.ws && j < a.we && m2 > best) best = m2;
+        }
+      }
+      tc_before_sync();
+      if (lane == 0) mbar_arrive(bar(tcw::B_FREE2 + k));
+#pragma unroll
+      for (int o = 8; o; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+      const int pr = R >> 4;
+      const long long pi = (ibeg + it) * PAIRS + pr;
+      if (pi < total && !*abort_flag) {
+        const int row = (int)pi;
+        if (a.coarse_out) {
+          if ((lane & 15) == 0) a.coarse_out[row] = sqrtf(best);
+        } else {
+          const bool fire = best > a.t2 && sqrtf(best) >= a.gate;
+          if (fire) {
+            if ((lane & 15) == 0) a.fire_list[atomicAdd(a.fire_count, 1)] = row;
           } else {
-            const bool fire = best > a.t2 && sqrtf(best) >= a.gate;
-            if (fire) {
-              if ((lane & 15) == 0) a.fire_list[atomicAdd(a.fire_count, 1)] = row;
-            } else {
-              const long long obase = (long long)row * a.full_nb;
-              for (int b = lane & 15; b < a.full_nb; b += 16) {
-                a.out_idx[(obase + b) * a.rs] = -1;
-                a.out_val[(obase + b) * a.rs] = make_float2(0.f, 0.f);
-              }
+            const long long obase = (long long)row * a.full_nb;
+            for (int b = lane & 15; b < a.full_nb; b += 16) {
+              a.out_idx[(obase + b) * a.rs] = -1;
+              a.out_val[(obase + b) * a.rs] = make_float2(0.f, 0.f);
             }
           }
         }
       }
     }
-    tc_before_sync();
-    __syncthreads();
-    tc_after_sync();
-    if (*abort_flag) break;
   }
+  tc_before_sync();
   __syncthreads();
+  tc_after_sync();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TMEM_COLS));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(tcw::TMEM_COLS));
 }
 
 // ------------------------------------------------------------------- host side
@@ -467,31 +523,21 @@ int tc_coarse_create(TcCoarse **out, int m, int ntmpl, int ndata, int fp16) {
   if (e == cudaSuccess) e = cudaMalloc(&c->err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->err, 0, sizeof(int));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(coarse_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+    e = cudaFuncSetAttribute(coarse_tc_ws_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, tcw::SMEM_BYTES);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(coarse_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(coarse_tc_kernel<0>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(coarse_tc_kernel<1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  int dev = 0, sms = 0, blocks = 0, smem_sm = 0;
+    e = cudaFuncSetAttribute(coarse_tc_ws_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tcw::SMEM_BYTES);
+  int dev = 0, sms = 0, smem_sm = 0;
   if (e == cudaSuccess) e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-  if (e == cudaSuccess) {
-    // Resident CTAs per SM from shared memory (1 KB per block is reserved by
-    // the driver) and from registers (launch bounds guarantee 2).
-    blocks = smem_sm / (tc::SMEM_BYTES + 1024);
-    if (blocks > 2) blocks = 2;
-  }
-  if (e != cudaSuccess || blocks < 1) {
+  if (e != cudaSuccess || smem_sm < tcw::SMEM_BYTES + 1024) {
     g_tc_err = e != cudaSuccess ? cudaGetErrorString(e) : "coarse kernel cannot be resident";
     tc_coarse_destroy(c);
     return -1;
   }
-  // TMEM: 128 columns per CTA, so at most 4 CTAs share an SM's 512 columns.
-  c->grid = sms * (blocks < 4 ? blocks : 4);
-  c->blocks_per_sm = blocks;
+  // One 512-thread CTA per SM (all 128 registers x 512 threads; 256 TMEM columns).
+  c->grid = sms;
+  c->blocks_per_sm = 1;
   *out = c;
   return 0;
 }
@@ -525,8 +571,8 @@ int tc_coarse_run(TcCoarse *c, const TcRunArgs &r, cudaStream_t s) {
   a.fire_count = r.fire_count;
   a.coarse_out = r.coarse_out;
   a.err = c->err;
-  if (c->fp16) coarse_tc_kernel<1><<<c->grid, tc::THREADS, tc::SMEM_BYTES, s>>>(a);
-  else coarse_tc_kernel<0><<<c->grid, tc::THREADS, tc::SMEM_BYTES, s>>>(a);
+  if (c->fp16) coarse_tc_ws_kernel<1><<<c->grid, tcw::THREADS, tcw::SMEM_BYTES, s>>>(a);
+  else coarse_tc_ws_kernel<0><<<c->grid, tcw::THREADS, tcw::SMEM_BYTES, s>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { g_tc_err = cudaGetErrorString(e); return -1; }
   return 0;
