@@ -72,7 +72,7 @@ __device__ __forceinline__ void large_pair(const LargeArgs &a, long long pi, int
 }
 
 template <int N2>
-__global__ void __launch_bounds__(N2 >= 256 ? N2 : 256)
+__global__ void __launch_bounds__(N2 >= 256 ? N2 : 256, N2 >= 1024 ? 1 : (N2 >= 512 ? 2 : 3))
 large_pass_a(const LargeArgs a) {
   constexpr int T2 = N2 / 16, C = LARGE_COLS;
   static_assert(T2 * C == N2, "pass A runs one thread per (column, point group)");

@@ -188,7 +188,8 @@ extern "C" int mfb_supported(size_t n) {
 static bool is_large(size_t n) { return n > 16384; }
 
 // ------------------------------------------------------------ large-n setup
-// n = N1 * N2 with N2 = 2^ceil(log2(n)/2) (<= 1024, the pass-A CTA size).
+// n = N1 * N2 with N2 = 2^ceil(log2(n)/2) (<= 1024, the pass-A CTA size; two
+// pass-A CTAs per SM at N2 = 512).
 struct LargeConst {
   int N1 = 0, N2 = 0, lo_bits = 0;
   float2 *tw_hi = nullptr, *tw_lo = nullptr;
