@@ -35,6 +35,26 @@ sys.path.insert(0, ROOT)
 N, ND, NT, BINSIZE, BAND = 4096, 16, 1024, 256, 512
 SNR, FD, THRESHOLD = 5.5, 1e-2, 5.5
 FLOPS_PER_PAIR = lambda n: 5 * n * int(np.log2(n)) + 9 * n   # the reference's own convention
+# Tensor-core flops the coarse pass executes per pair at band 512: per 8 pairs,
+# stage 1 = 12 MMAs of M128 x N32 x K16 and stage 2 = 12 MMAs of M128 x N64 x K16
+# (hi*hi + hi*lo + lo*hi included), 2 flops per multiply-add.
+TC_FLOPS_PER_PAIR = (12 * 128 * 32 * 16 * 2 + 12 * 128 * 64 * 16 * 2) / 8
+# DRAM bytes per launch from one ncu capture of the same kernels on this workload
+# (profiles/coarse_tc_ws_band512_16x1024.md, profiles/flat_kernel_n4096_16x1024.md).
+TRAFFIC_COARSE_TC = 4.347e6
+TRAFFIC_FLAT = 34.18e6
+
+
+def measured_peaks():
+    """(bf16 TFLOP/s, HBM GB/s, source) from MEASURED_PEAKS.json, else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["bf16_tflops"]), float(m["hbm_gbs"]), "MEASURED_PEAKS.json (burst)"
+    except (OSError, ValueError, KeyError):
+        return 1590.0, 6650.0, "fallback (no MEASURED_PEAKS.json)"
+
+
 METRIC = "filter pairs/sec at n=4096: mixed-precision hier vs FP32 flat, same FD rate"
 WORKLOAD = ("hierarchical n=4096 ndata=16 ntemplates=1024 binsize=256 band=512 snr=5.5 "
             "fd=1e-2 threshold=5.5, 10% of segments injected at SNR U[5,12]")
@@ -376,6 +396,27 @@ def our_arm(args):
     dominant = "coarse" if coarse_ms >= refine_ms else "refine"
     dom_flops, dom_ms = (coarse_flops, coarse_ms) if dominant == "coarse" else (refine_flops,
                                                                                 refine_ms)
+    bf16_peak, hbm_peak, peak_src = measured_peaks()
+    if dominant == "coarse" and args.coarse != "fp32":
+        tc_flops = rows * TC_FLOPS_PER_PAIR
+        roofline_line = {
+            "bound": "tensor", "kernel": "coarse_tc_ws_kernel",
+            "achieved": tc_flops / (coarse_ms * 1e-3) / 1e12, "peak": bf16_peak,
+            "unit": "TFLOP/s", "frac": tc_flops / (coarse_ms * 1e-3) / (bf16_peak * 1e12),
+            "traffic": TRAFFIC_COARSE_TC,
+            "flops_per_pair": TC_FLOPS_PER_PAIR,
+            "hbm_frac": TRAFFIC_COARSE_TC / (coarse_ms * 1e-3) / (hbm_peak * 1e9),
+            "fp32_equivalent": {"achieved": coarse_flops / (coarse_ms * 1e-3) / 1e12,
+                                "frac": coarse_flops / (coarse_ms * 1e-3) / peak.value,
+                                "flops_per_pair": FLOPS_PER_PAIR(BAND)},
+            "peak_source": "bf16 dense GEMM " + peak_src + "; traffic from an ncu capture"}
+    else:
+        roofline_line = {
+            "bound": "fp32", "kernel": dominant,
+            "achieved": dom_flops / (dom_ms * 1e-3) / 1e12, "peak": peak.value / 1e12,
+            "unit": "TFLOP/s", "frac": dom_flops / (dom_ms * 1e-3) / peak.value,
+            "traffic": TRAFFIC_FLAT if dominant == "refine" else None,
+            "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak)"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
@@ -396,16 +437,15 @@ def our_arm(args):
                            "ms_per_step": model_ms_step, "refine_rate": trig_mod / rows,
                            "speedup_vs_flat": model_value / flat_value},
             "kernels_ms": {"coarse_gate": coarse_ms, "refine": refine_ms},
-            "roofline": {"bound": "fp32", "kernel": dominant,
-                         "achieved": dom_flops / (dom_ms * 1e-3) / 1e12,
-                         "peak": peak.value / 1e12, "unit": "TFLOP/s",
-                         "frac": dom_flops / (dom_ms * 1e-3) / peak.value, "traffic": None,
-                         "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak)"},
+            "roofline": roofline_line,
             "roofline_flat": {"bound": "fp32", "achieved": flat_achieved,
                               "peak": peak.value / 1e12, "unit": "TFLOP/s",
                               "frac": flat_achieved * 1e12 / peak.value,
                               "flops_per_pair": FLOPS_PER_PAIR(N),
-                              "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak)"},
+                              "traffic": TRAFFIC_FLAT,
+                              "hbm_frac": TRAFFIC_FLAT / (flat_ms_step * 1e-3) / (hbm_peak * 1e9),
+                              "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak); "
+                                             "traffic from an ncu capture"},
             "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": ND * N * 8,
                     "d2h_bytes_per_step": rows * nb * 16},
             "gpu_launches": 3 * args.steps,
