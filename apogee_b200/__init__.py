@@ -176,7 +176,7 @@ class MatchedFilter:
         """Reused device (or pinned host) tensor for outputs."""
         torch = _torch()
         b = self._bufs.get(key)
-        numel = int(np.prod(shape))
+        numel = math.prod(shape)
         if b is None or b.numel() < numel or b.dtype != dtype:
             if pinned:
                 b = torch.empty(max(numel, 1), dtype=dtype, pin_memory=True)
@@ -507,6 +507,8 @@ class HierarchicalFilter(MatchedFilter):
         self._gate_cache = None
         self._pairs0 = 0
         self._trig0 = 0
+        self._table = None     # pinned host table the device writes (run())
+        self.last_d2h_bytes = 0
         torch = _torch()
         dev = torch.device("cuda", self.device.index)
         # Spectra are staged on the device until the band is known.
@@ -764,12 +766,41 @@ class HierarchicalFilter(MatchedFilter):
 
     def run(self, binsize=None, threshold=0.0, window=None,
             data=None, templates=None, counts=False, raw=False):
+        """Hierarchical run; the table as ``MatchedFilter.run``.
+
+        The default structured table is kept in pinned host memory between
+        calls and only the refined rows cross the host link (every row the
+        gate dismisses is all empty records), written by the device straight
+        into the host table: it is returned read-only and is updated in place
+        by the next call.
+        """
         binsize, start, end, d0, nd, t0, nt, nb = self._run_args(binsize, window, data, templates)
         threshold = float(threshold)
         if math.isnan(threshold):
             raise ValueError("threshold must not be NaN")
         self._prepare()
+        if not counts and not raw:
+            return self._run_host(binsize, threshold, start, end, d0, nd, t0, nt, nb)
         return self._run_common(binsize, threshold, start, end, d0, nd, t0, nt, nb, counts, raw)
+
+    def _run_host(self, binsize, threshold, start, end, d0, nd, t0, nt, nb):
+        torch = _torch()
+        stream = self._bind_stream()
+        need = nd * nt * nb * 2                   # int64 words of the table
+        rec_d = self._buffer("rec", (need,), torch.int64)
+        tab = self._table
+        if tab is None or tab.numel() < need:
+            tab = self._table = torch.empty(need, dtype=torch.int64, pin_memory=True)
+        info = self._buffer("info", (2,), torch.int64, pinned=True)
+        _lib.check(_lib.lib().mfb_hier_run_host(self._hplan, d0, nd, t0, nt, binsize, threshold,
+                                                start, end, rec_d.data_ptr(), tab.data_ptr(),
+                                                info.data_ptr()),
+                   "hierarchical filter failed")
+        stream.synchronize()
+        self.last_d2h_bytes = int(info.numpy()[1])
+        out = tab.numpy()[:need].view(PEAK_DTYPE).reshape(nd, nt, nb)
+        out.flags.writeable = False
+        return out
 
     def run_device(self, binsize=None, threshold=0.0, window=None, data=None, templates=None):
         torch = _torch()

@@ -71,6 +71,62 @@ inline cudaError_t launch_hier_scale(const HierScaleArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// The hierarchical run's table written straight into a caller's pinned host
+// table (mapped memory, stores over the host link).  Every row the gate
+// dismisses is all empty records (index -1, value 0), so when the host table
+// holds the previous run's result only the rows that change cross the link:
+// the rows refined last time go back to empty (unwrite), then the rows
+// refined now are copied from the device table (write), in that stream order.
+struct HierHostArgs {
+  const int4 *records;        // device table [rows][nb]
+  int4 *table;                // host table [rows][nb] (device-visible pointer)
+  long long nb;
+  const int32_t *list, *count;        // this run's refined rows
+  int32_t *prev_list, *prev_count;    // the rows the host table holds, updated here
+  unsigned long long *total;  // plan's trigger total
+  long long *info;            // host [2] (device-visible) or null: refined rows, bytes written
+  int write_rows;             // 0: the table was copied whole, only bookkeeping
+  long long full_bytes;       // bytes of that whole copy
+};
+
+static __global__ void hier_unwrite_kernel(const HierHostArgs a) {
+  const long long c = *a.prev_count;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const int4 empty = make_int4(-1, -1, 0, 0);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < c * a.nb; e += stride) {
+    const long long i = e / a.nb;
+    a.table[(long long)a.prev_list[i] * a.nb + (e - i * a.nb)] = empty;
+  }
+}
+
+static __global__ void hier_write_kernel(const HierHostArgs a) {
+  const long long c = *a.count;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (a.write_rows)
+    for (long long e = t0; e < c * a.nb; e += stride) {
+      const long long i = e / a.nb;
+      const long long at = (long long)a.list[i] * a.nb + (e - i * a.nb);
+      a.table[at] = a.records[at];
+    }
+  for (long long i = t0; i < c; i += stride) a.prev_list[i] = a.list[i];
+  if (t0 == 0) {
+    const long long pc = *a.prev_count;
+    *a.total += (unsigned long long)c;
+    *a.prev_count = (int32_t)c;
+    if (a.info) {
+      a.info[0] = c;
+      a.info[1] = a.write_rows ? (pc + c) * a.nb * 16 : a.full_bytes;
+    }
+  }
+}
+
+inline int hier_host_grid(long long max_elems, int sms) {
+  long long blocks = (max_elems + 255) / 256;
+  if (blocks > 2ll * sms) blocks = 2ll * sms;
+  return blocks < 1 ? 1 : (int)blocks;
+}
+
 static __global__ void reference_sum_kernel(const float *p, int n, int m, double *out) {
   double low = 0.0, total = 0.0;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {

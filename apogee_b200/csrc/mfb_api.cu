@@ -723,6 +723,11 @@ struct mfb_hplan {
   unsigned long long *trig_total = nullptr;  // device: survivors summed over runs
   long long pairs = 0;
   TcCoarse *tc = nullptr;       // tensor-core coarse state
+  // mfb_hier_run_host: the rows refined in the host table it last wrote
+  int32_t *prev_list = nullptr; // [nd*nt]
+  int32_t *prev_count = nullptr;
+  const void *host_table = nullptr;
+  long long host_rows = -1, host_nb = -1;
 };
 
 extern "C" int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, size_t band,
@@ -751,6 +756,9 @@ extern "C" int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, 
     if (e == cudaSuccess) e = cudaMalloc(&h->fire_list, (size_t)ndata * ntmpl * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&h->fire_count, sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&h->trig_total, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&h->prev_list, (size_t)ndata * ntmpl * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&h->prev_count, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(h->prev_count, 0, sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMemset(h->trig_total, 0, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(h->ct, 0, (size_t)ntmpl * band * sizeof(float2));
     if (e == cudaSuccess) e = cudaMemset(h->fpow, 0, (size_t)ntmpl * sizeof(float));
@@ -779,6 +787,8 @@ extern "C" int mfb_hier_destroy(mfb_hplan *h) {
   cudaFree(h->fire_list);
   cudaFree(h->fire_count);
   cudaFree(h->trig_total);
+  cudaFree(h->prev_list);
+  cudaFree(h->prev_count);
   free(h->tready);
   tc_coarse_destroy(h->tc);
   delete h;
@@ -886,7 +896,8 @@ __global__ void accumulate_triggers(const int32_t *count, unsigned long long *to
 
 static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t binsize,
                          float threshold, size_t start, size_t end, int64_t *idx, void *val,
-                         int32_t *counts, int rs, int phase = 0) {
+                         int32_t *counts, int rs, int phase = 0, void *table = nullptr,
+                         long long *info = nullptr) {
   if (!h) return fail(MFB_ERR_ARG, "null plan");
   mfb_plan *p = h->full;
   size_t nb;
@@ -947,8 +958,40 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
   r = run_rows_impl(p, d0, nd, t0, nt, h->fire_list, h->fire_count, nd * nt, binsize, threshold,
                     start, end, idx, val, counts, rs);
   if (r) return r;
-  accumulate_triggers<<<1, 1, 0, s>>>(h->fire_count, h->trig_total);
-  CUDA_TRY(cudaGetLastError());
+  if (table) {
+    // table, info: device-visible pointers of the caller's pinned host memory
+    const long long rows = (long long)nd * nt;
+    HierHostArgs ha;
+    ha.records = (const int4 *)idx;
+    ha.table = (int4 *)table;
+    ha.nb = (long long)nb;
+    ha.list = h->fire_list;
+    ha.count = h->fire_count;
+    ha.prev_list = h->prev_list;
+    ha.prev_count = h->prev_count;
+    ha.total = h->trig_total;
+    ha.info = info;
+    ha.full_bytes = rows * (long long)nb * 16;
+    const bool same = table == h->host_table && rows == h->host_rows && (long long)nb == h->host_nb;
+    ha.write_rows = same ? 1 : 0;
+    int sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    const int grid = hier_host_grid(rows * (long long)nb, sms);
+    if (same) {
+      hier_unwrite_kernel<<<grid, 256, 0, s>>>(ha);
+      CUDA_TRY(cudaGetLastError());
+    } else {
+      CUDA_TRY(cudaMemcpyAsync(table, idx, (size_t)ha.full_bytes, cudaMemcpyDefault, s));
+    }
+    hier_write_kernel<<<grid, 256, 0, s>>>(ha);
+    CUDA_TRY(cudaGetLastError());
+    h->host_table = table;
+    h->host_rows = rows;
+    h->host_nb = (long long)nb;
+  } else {
+    accumulate_triggers<<<1, 1, 0, s>>>(h->fire_count, h->trig_total);
+    CUDA_TRY(cudaGetLastError());
+  }
   h->pairs += (long long)nd * nt;
   return MFB_OK;
 }
@@ -973,6 +1016,29 @@ extern "C" int mfb_hier_run_records(mfb_hplan *h, int d0, int nd, int t0, int nt
   if (!records) return fail(MFB_ERR_ARG, "null output");
   return hier_run_impl(h, d0, nd, t0, nt, binsize, threshold, start, end, (int64_t *)records,
                        (char *)records + 8, counts, 2);
+}
+
+extern "C" int mfb_hier_run_host(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t binsize,
+                                 float threshold, size_t start, size_t end, void *records,
+                                 void *table, int64_t *info) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  if (!records || !table) return fail(MFB_ERR_ARG, "null output");
+  if (((uintptr_t)records | (uintptr_t)table) & 15)
+    return fail(MFB_ERR_ARG, "records and table must be 16-byte aligned");
+  DeviceGuard dg(h->device);
+  void *dtab = nullptr, *dinfo = nullptr;
+  if (cudaHostGetDevicePointer(&dtab, table, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MFB_ERR_ARG, "table must be pinned (page-locked, mapped) host memory");
+  }
+  if (info && cudaHostGetDevicePointer(&dinfo, info, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MFB_ERR_ARG, "info must be pinned (page-locked, mapped) host memory");
+  }
+  int r = hier_run_impl(h, d0, nd, t0, nt, binsize, threshold, start, end, (int64_t *)records,
+                        (char *)records + 8, nullptr, 2, 0, dtab, (long long *)dinfo);
+  if (r) h->host_table = nullptr;
+  return r;
 }
 
 extern "C" int mfb_hier_coarse_values(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t start,

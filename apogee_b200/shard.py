@@ -54,6 +54,8 @@ def all_gather_peaks(local, nt_total, group=None):
     backend = dist.get_backend(group)
     dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" \
         else torch.device("cpu")
+    if not local.flags.writeable:               # a hierarchical run's host table
+        local = local.copy()
     words = torch.from_numpy(local.view(np.int64).reshape(nd, cnt, nb * 2))
     padded = torch.zeros(nd, maxc, nb * 2, dtype=torch.int64, device=dev)
     padded[:, :cnt] = words.to(dev)

@@ -131,6 +131,23 @@ int mfb_hier_run(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t binsize, f
 int mfb_hier_run_records(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t binsize,
                          float threshold, size_t start, size_t end, void *records,
                          int32_t *counts);
+/* mfb_hier_run_records whose table lands in the caller's HOST memory.
+   records: DEVICE workspace of nd*nt*nb 16-byte records (16-byte aligned),
+   left holding the table as mfb_hier_run_records writes it.  table: pinned,
+   mapped host memory (cudaHostAlloc / cudaMallocHost / cudaHostRegister) of
+   nd*nt*nb records, written by the device on the plan's stream.  Every row
+   the gate dismisses is all empty records (index -1, value 0), so when
+   `table` is the one this plan wrote last with the same nd*nt and nb, only
+   the rows that change cross the host link: the rows refined last time are
+   reset to empty, then the rows refined now are written.  Any other table is
+   copied whole.  The caller must not write into the table between calls.
+   info: pinned host int64[2] or NULL; receives the refined rows and the
+   bytes written into the table.  Read table and info after synchronising
+   the stream.  The plan's trigger total is updated as by mfb_hier_run.
+   Same contract as ap_hmf_run (src/hmf.c:222-328) for the table itself. */
+int mfb_hier_run_host(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t binsize,
+                      float threshold, size_t start, size_t end, void *records, void *table,
+                      int64_t *info);
 /* mfb_hier_run split for measurement: phase 1 enqueues only the coarse pass
    and gate (dismissed rows written, survivor list built), phase 2 only the
    refine of the list phase 1 built; phase 0 is the whole run.  Lets a caller

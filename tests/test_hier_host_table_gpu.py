@@ -1,0 +1,133 @@
+"""HierarchicalFilter.run writes its table from the device straight into a
+pinned host table (mfb_hier_run_host): only the rows that change since the
+previous call cross the host link.  Every call must equal the dense table
+of the same run (mfb_hier_run, raw output), whatever the previous call left
+in the host table."""
+import numpy as np
+import pytest
+
+from oracle import oracle, parity
+
+pytestmark = pytest.mark.gpu
+
+
+def noise(rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+def _filter(n, nd, nt, band, coarse, gate):
+    import apogee_b200 as mf
+    hf = mf.HierarchicalFilter(n, nd, nt, band=band, coarse=coarse)
+    hf.set_coarse_threshold(gate)
+    return hf
+
+
+def _dense(hf, **kw):
+    idx, val = hf.run(raw=True, **kw)
+    return idx.copy(), val.copy()
+
+
+@pytest.mark.parametrize("coarse", ["fp32", "bf16x3"])
+def test_packed_equals_dense_over_changing_survivors(coarse):
+    n, nd, nt, band, bs, thr = 4096, 4, 64, 512, 256, 330.0
+    rng = np.random.default_rng(11)
+    H = noise(rng, (nt, n))
+    hf = _filter(n, nd, nt, band, coarse, 0.0)
+    hf.set_templates(H)
+    hf.set_data(noise(rng, (nd, n)))
+    # a gate that about one pair in ten passes
+    hf.set_coarse_threshold(float(np.quantile(hf.coarse_values(), 0.9)))
+    seen = set()
+    for _ in range(6):
+        D = noise(rng, (nd, n))
+        hf.set_data(D)
+        out = hf.run(binsize=bs, threshold=thr)
+        seen.add(hf.last_refinements)
+        idx, val = _dense(hf, binsize=bs, threshold=thr)
+        assert out.shape == (nd, nt, n // bs)
+        np.testing.assert_array_equal(out["index"], idx)
+        np.testing.assert_array_equal(out["value"], val)
+        hit = (out["index"] >= 0).any(-1)
+        assert 0 < hit.sum() < nd * nt
+        bad = parity.compare(out["index"], out["value"], oracle.correlate(D, H), bs, thr,
+                             rows_mask=hit)
+        assert not bad, bad[:3]
+    assert len(seen) > 1                          # the survivor sets really changed
+
+
+def test_packed_gate_extremes_and_shape_changes():
+    n, nd, nt, band = 4096, 3, 40, 512
+    rng = np.random.default_rng(12)
+    H = noise(rng, (nt, n))
+    D = noise(rng, (nd, n))
+    hf = _filter(n, nd, nt, band, "bf16x3", 0.0)
+    hf.set_templates(H)
+    hf.set_data(D)
+    z = oracle.correlate(D, H)
+    # gate 0: every row refines, more than the first prefix guess (256 rows)
+    big = _filter(n, 8, 64, band, "bf16x3", 0.0)
+    Hb, Db = noise(rng, (64, n)), noise(rng, (8, n))
+    big.set_templates(Hb)
+    big.set_data(Db)
+    out = big.run(binsize=512)
+    assert big.last_refinements == 8 * 64
+    bad = parity.compare(out["index"], out["value"], oracle.correlate(Db, Hb), 512, 0.0)
+    assert not bad, bad[:3]
+    # all rows refine, then none: the host copy must drop every old row
+    a = hf.run(binsize=256, threshold=0.0)
+    assert not parity.compare(a["index"], a["value"], z, 256, 0.0)
+    hf.set_coarse_threshold(1e30)
+    b = hf.run(binsize=256, threshold=0.0)
+    assert hf.last_refinements == 0
+    assert (b["index"] == -1).all() and (b["value"] == 0).all()
+    # a window and a sub-block change the table's shape; then back again
+    hf.set_coarse_threshold(0.0)
+    c = hf.run(binsize=300, threshold=0.0, window=(100, 3000), data=(1, 2), templates=(5, 30))
+    idx, val = _dense(hf, binsize=300, threshold=0.0, window=(100, 3000), data=(1, 2),
+                      templates=(5, 30))
+    np.testing.assert_array_equal(c["index"], idx)
+    np.testing.assert_array_equal(c["value"], val)
+    d = hf.run(binsize=256, threshold=0.0)
+    assert not parity.compare(d["index"], d["value"], z, 256, 0.0)
+
+
+def test_packed_result_is_read_only():
+    n, nd, nt = 4096, 2, 8
+    rng = np.random.default_rng(13)
+    hf = _filter(n, nd, nt, 512, "fp32", 0.0)
+    hf.set_templates(noise(rng, (nt, n)))
+    hf.set_data(noise(rng, (nd, n)))
+    out = hf.run(binsize=1024)
+    with pytest.raises(ValueError):
+        out["index"][0, 0, 0] = 5
+    keep = out.copy()
+    keep["index"][0, 0, 0] = 5                    # a copy is the caller's
+
+
+def test_host_table_bytes_and_unpinned_table_rejected():
+    import ctypes
+    from apogee_b200 import _lib
+    n, nd, nt, nb = 4096, 2, 16, 4
+    rng = np.random.default_rng(14)
+    hf = _filter(n, nd, nt, 512, "bf16x3", 0.0)
+    hf.set_templates(noise(rng, (nt, n)))
+    hf.set_data(noise(rng, (nd, n)))
+    hf.run(binsize=n // nb)
+    full = nd * nt * nb * 16
+    assert hf.last_d2h_bytes == full              # a new table is copied whole
+    hf.run(binsize=n // nb)
+    assert hf.last_d2h_bytes == 2 * full          # every row reset, then written again
+    hf.set_coarse_threshold(1e30)
+    hf.run(binsize=n // nb)
+    assert hf.last_d2h_bytes == full              # reset only
+    hf.run(binsize=n // nb)
+    assert hf.last_d2h_bytes == 0                 # nothing changes
+    # a pageable host table is refused before anything is enqueued
+    import torch
+    rec = torch.empty(nd * nt * nb * 2, dtype=torch.int64, device="cuda")
+    pageable = np.empty(nd * nt * nb * 2 + 2, np.int64)
+    ptr = (pageable.ctypes.data + 15) // 16 * 16
+    L = _lib.lib()
+    rc = L.mfb_hier_run_host(hf._hplan, 0, nd, 0, nt, n // nb, 0.0, 0, n, rec.data_ptr(),
+                             ctypes.c_void_p(ptr), None)
+    assert rc == -1 and b"pinned" in L.mfb_last_error()
