@@ -509,6 +509,8 @@ class HierarchicalFilter(MatchedFilter):
         self._trig0 = 0
         self._table = None     # pinned host table the device writes (run())
         self.last_d2h_bytes = 0
+        self._hostdata = None  # host data bank, read by the device at run()
+        self._upload_evt = None
         torch = _torch()
         dev = torch.device("cuda", self.device.index)
         # Spectra are staged on the device until the band is known.
@@ -552,14 +554,36 @@ class HierarchicalFilter(MatchedFilter):
             _lib.check(_lib.lib().mfb_hier_set_stream(self._hplan, s.cuda_stream))
         return s
 
+    def _release_hostdata(self):
+        """Drop the held host bank once no upload from it is in flight."""
+        if self._upload_evt is not None:
+            self._upload_evt.synchronize()
+            self._upload_evt = None
+        self._hostdata = None
+
     def set_data(self, spectra, index=None):
+        """Set all data spectra (or one, with ``index``).
+
+        A host bank is held, not copied: the device reads it when run()
+        needs it, in stream order ahead of the kernels (the reference's CPU
+        engine also keeps the caller's array and reads it during run,
+        python/matchedfilter/__init__.py:335-351), so do not change the array
+        before run() has returned.  From pinned memory the upload is one
+        asynchronous copy with no host synchronisation.
+        """
         index = self._input_index(index, self.ndata)
         torch = _torch()
         if index is None:
             s = _Spectra(spectra, (self.ndata, self.n), self.device.index)
-            src = s.keep if _is_torch(s.keep) else torch.from_numpy(s.keep)
-            self._gd.copy_(src)
+            self._release_hostdata()
+            if _is_torch(s.keep):
+                self._gd.copy_(s.keep)
+            else:
+                self._hostdata = s.keep
         else:
+            if self._hostdata is not None:          # the device mirror takes the bank first
+                self._gd.copy_(torch.from_numpy(self._hostdata))
+                self._release_hostdata()
             a = spectra
             if not (_is_torch(a) and a.is_cuda):
                 a = np.ascontiguousarray(_host_array(a), dtype=np.complex64)
@@ -639,7 +663,14 @@ class HierarchicalFilter(MatchedFilter):
                 self._hplan, None if ref is None else ref.ctypes.data))
             self._tdirty = False
         if self._ddirty:
-            _lib.check(L.mfb_hier_set_data(self._hplan, 0, self.ndata, self._gd.data_ptr()))
+            if self._hostdata is not None:
+                _lib.check(L.mfb_hier_set_data(self._hplan, 0, self.ndata,
+                                               self._hostdata.ctypes.data))
+                if self._upload_evt is None:
+                    self._upload_evt = _torch().cuda.Event()
+                self._upload_evt.record(self._stream())
+            else:
+                _lib.check(L.mfb_hier_set_data(self._hplan, 0, self.ndata, self._gd.data_ptr()))
             self._ddirty = False
         if not self._thr_applied:
             _lib.check(L.mfb_hier_set_threshold(self._hplan, self._coarse_value(band)))

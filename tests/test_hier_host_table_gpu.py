@@ -131,3 +131,30 @@ def test_host_table_bytes_and_unpinned_table_rejected():
     rc = L.mfb_hier_run_host(hf._hplan, 0, nd, 0, nt, n // nb, 0.0, 0, n, rec.data_ptr(),
                              ctypes.c_void_p(ptr), None)
     assert rc == -1 and b"pinned" in L.mfb_last_error()
+
+
+def test_held_host_bank_then_row_update():
+    """set_data keeps a host bank and the device reads it at run(); a later
+    single-row set_data lands on top of that bank."""
+    import torch
+    n, nd, nt, bs = 4096, 3, 8, 1024
+    rng = np.random.default_rng(15)
+    H = noise(rng, (nt, n))
+    A = noise(rng, (nd, n))
+    hf = _filter(n, nd, nt, 512, "bf16x3", 0.0)
+    hf.set_templates(H)
+    pin = torch.empty((nd, n), dtype=torch.complex64, pin_memory=True)
+    pin.numpy()[:] = A
+    hf.set_data(pin.numpy())                     # pinned: one asynchronous upload at run()
+    out = hf.run(binsize=bs)
+    assert not parity.compare(out["index"], out["value"], oracle.correlate(A, H), bs)
+    B = noise(rng, (n,))
+    hf.set_data(B, index=1)
+    A2 = A.copy()
+    A2[1] = B
+    out = hf.run(binsize=bs)
+    assert not parity.compare(out["index"], out["value"], oracle.correlate(A2, H), bs)
+    C = noise(rng, (nd, n))
+    hf.set_data(C.astype(np.complex128))         # converted: the filter holds its own copy
+    out = hf.run(binsize=bs)
+    assert not parity.compare(out["index"], out["value"], oracle.correlate(C, H), bs)
