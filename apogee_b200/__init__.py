@@ -145,6 +145,7 @@ class MatchedFilter:
         self._data_ready = set()
         self._template_ready = set()
         self._bufs = {}
+        self._views = {}
         self._plan = None
 
     def _create_plan(self):
@@ -174,6 +175,9 @@ class MatchedFilter:
 
     def _buffer(self, key, shape, dtype, pinned=False):
         """Reused device (or pinned host) tensor for outputs."""
+        v = self._views.get((key, shape, dtype))
+        if v is not None:
+            return v
         torch = _torch()
         b = self._bufs.get(key)
         numel = math.prod(shape)
@@ -184,7 +188,10 @@ class MatchedFilter:
                 b = torch.empty(max(numel, 1), dtype=dtype,
                                 device=torch.device("cuda", self.device.index))
             self._bufs[key] = b
-        return b[:numel].view(*shape)
+            self._views = {k: w for k, w in self._views.items() if k[0] != key}
+        v = b[:numel].view(*shape)
+        self._views[(key, shape, dtype)] = v
+        return v
 
     # ---- ingest ---------------------------------------------------------------
     def _input_index(self, index, size):
@@ -650,11 +657,13 @@ class HierarchicalFilter(MatchedFilter):
         self._gate_cache = (key, float(v))
         return float(v)
 
-    def _prepare(self):
+    def _prepare(self, defer_host=False):
+        """Build the plan and push pending state; with defer_host a held host
+        data bank is left for the run call to upload (returns its address)."""
         band = self._choose_band()
         self._build(band)
         L = _lib.lib()
-        self._bind_stream()
+        self._cur_stream = self._bind_stream()
         if self._tdirty:
             _lib.check(L.mfb_hier_set_templates(self._hplan, 0, self.ntemplates,
                                                 self._gt.data_ptr()))
@@ -662,20 +671,24 @@ class HierarchicalFilter(MatchedFilter):
             _lib.check(L.mfb_hier_set_reference(
                 self._hplan, None if ref is None else ref.ctypes.data))
             self._tdirty = False
+        host = None
+        if not self._thr_applied:
+            _lib.check(L.mfb_hier_set_threshold(self._hplan, self._coarse_value(band)))
+            self._thr_applied = True
         if self._ddirty:
-            if self._hostdata is not None:
+            if self._hostdata is not None and defer_host:
+                host = self._hostdata.ctypes.data
+            elif self._hostdata is not None:
                 _lib.check(L.mfb_hier_set_data(self._hplan, 0, self.ndata,
                                                self._hostdata.ctypes.data))
                 if self._upload_evt is None:
                     self._upload_evt = _torch().cuda.Event()
                 self._upload_evt.record(self._stream())
+                self._ddirty = False
             else:
                 _lib.check(L.mfb_hier_set_data(self._hplan, 0, self.ndata, self._gd.data_ptr()))
-            self._ddirty = False
-        if not self._thr_applied:
-            _lib.check(L.mfb_hier_set_threshold(self._hplan, self._coarse_value(band)))
-            self._thr_applied = True
-        return band
+                self._ddirty = False
+        return host
 
     def set_coarse_threshold(self, value):
         """Pin the coarse threshold (requires a pinned band); None -> model."""
@@ -809,14 +822,15 @@ class HierarchicalFilter(MatchedFilter):
         threshold = float(threshold)
         if math.isnan(threshold):
             raise ValueError("threshold must not be NaN")
-        self._prepare()
         if not counts and not raw:
-            return self._run_host(binsize, threshold, start, end, d0, nd, t0, nt, nb)
+            host = self._prepare(defer_host=True)
+            return self._run_host(binsize, threshold, start, end, d0, nd, t0, nt, nb, host)
+        self._prepare()
         return self._run_common(binsize, threshold, start, end, d0, nd, t0, nt, nb, counts, raw)
 
-    def _run_host(self, binsize, threshold, start, end, d0, nd, t0, nt, nb):
+    def _run_host(self, binsize, threshold, start, end, d0, nd, t0, nt, nb, host=None):
         torch = _torch()
-        stream = self._bind_stream()
+        stream = self._cur_stream                 # bound by _prepare
         need = nd * nt * nb * 2                   # int64 words of the table
         rec_d = self._buffer("rec", (need,), torch.int64)
         tab = self._table
@@ -824,10 +838,12 @@ class HierarchicalFilter(MatchedFilter):
             tab = self._table = torch.empty(need, dtype=torch.int64, pin_memory=True)
         info = self._buffer("info", (2,), torch.int64, pinned=True)
         _lib.check(_lib.lib().mfb_hier_run_host(self._hplan, d0, nd, t0, nt, binsize, threshold,
-                                                start, end, rec_d.data_ptr(), tab.data_ptr(),
-                                                info.data_ptr()),
+                                                start, end, host, rec_d.data_ptr(),
+                                                tab.data_ptr(), info.data_ptr()),
                    "hierarchical filter failed")
         stream.synchronize()
+        if host is not None:
+            self._ddirty = False
         self.last_d2h_bytes = int(info.numpy()[1])
         out = tab.numpy()[:need].view(PEAK_DTYPE).reshape(nd, nt, nb)
         out.flags.writeable = False

@@ -87,7 +87,7 @@ SIGNATURES = {
     "mfb_hier_set_threshold": (_I, [_P, _F]),
     "mfb_hier_run": (_I, [_P, _I, _I, _I, _I, _SZ, _F, _SZ, _SZ, _P, _P, _P]),
     "mfb_hier_run_records": (_I, [_P, _I, _I, _I, _I, _SZ, _F, _SZ, _SZ, _P, _P]),
-    "mfb_hier_run_host": (_I, [_P, _I, _I, _I, _I, _SZ, _F, _SZ, _SZ, _P, _P, _P]),
+    "mfb_hier_run_host": (_I, [_P, _I, _I, _I, _I, _SZ, _F, _SZ, _SZ, _P, _P, _P, _P]),
     "mfb_hier_run_phase": (_I, [_P, _I, _I, _I, _I, _I, _SZ, _F, _SZ, _SZ, _P, _P, _P]),
     "mfb_hier_last_triggers": (_I, [_P, _I64P]),
     "mfb_hier_stats": (_I, [_P, _I64P, _I64P]),

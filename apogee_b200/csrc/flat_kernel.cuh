@@ -759,4 +759,23 @@ flat_kernel(const FlatArgs a) {
   }
 }
 
+// Listed mode on its own: the output rows of a device row list (the
+// hierarchical refine, mfb_run_rows).  Survivor lists are short and in
+// arbitrary order, so the run is latency bound (a few pairs per CTA, each
+// loading its own data row): without the data-row cache the kernel fits in
+// 80 registers and three 256-thread CTAs per SM, 444 pairs in flight instead
+// of 296 on 148 SMs.
+template <int N>
+__global__ void __launch_bounds__(FlatGeo<N>::CTA, FlatGeo<N>::CTA <= 256 ? 3 : 1)
+rows_kernel(const FlatArgs a) {
+  using Geo = FlatGeo<N>;
+  extern __shared__ __align__(16) float2 smem[];
+  const long long total = *a.list_count;
+  const long long items = (total + Geo::G - 1) / Geo::G;
+  const long long per = items / gridDim.x, extra = items % gridDim.x;
+  const long long ibeg = blockIdx.x * per + (blockIdx.x < extra ? blockIdx.x : extra);
+  const long long iend = ibeg + per + (blockIdx.x < extra ? 1 : 0);
+  flat_range<N, MODE_PEAKS, false>(a, ibeg, iend, smem);
+}
+
 }  // namespace mfb

@@ -98,6 +98,7 @@ struct NConst {
   float2 *twid = nullptr;
   int grid_peaks = 0, grid_gate = 0, grid_fwd = 0;
   int cta = 0, smem = 0, g = 0;
+  int grid_rows = 0;
 };
 static std::mutex g_const_mu;
 static std::map<std::pair<int, int>, NConst> g_const;
@@ -117,7 +118,9 @@ static int make_const(int device, NConst &c) {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, Geo::SMEM));
   CUDA_TRY(cudaFuncSetAttribute(series_forward_kernel<N>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, Geo::SMEM));
-  int sms = 0, b1 = 0, b2 = 0, b3 = 0;
+  CUDA_TRY(cudaFuncSetAttribute(rows_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Geo::SMEM));
+  int sms = 0, b1 = 0, b2 = 0, b3 = 0, b4 = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, flat_kernel<N, MODE_PEAKS>,
                                                          Geo::CTA, Geo::SMEM));
@@ -125,8 +128,11 @@ static int make_const(int device, NConst &c) {
                                                          Geo::CTA, Geo::SMEM));
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, series_forward_kernel<N>,
                                                          Geo::CTA, Geo::SMEM));
-  if (b1 < 1 || b2 < 1 || b3 < 1)
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, rows_kernel<N>, Geo::CTA,
+                                                         Geo::SMEM));
+  if (b1 < 1 || b2 < 1 || b3 < 1 || b4 < 1)
     return fail(MFB_ERR_CUDA, "kernel for n=%d cannot be resident on this device", N);
+  c.grid_rows = b4 * sms;
   c.grid_peaks = b1 * sms;
   c.grid_gate = b2 * sms;
   c.grid_fwd = b3 * sms;
@@ -162,6 +168,17 @@ static cudaError_t launch_flat(int n, const NConst &c, const FlatArgs &a, cudaSt
   const int grid = MODE == MODE_PEAKS ? c.grid_peaks : c.grid_gate;
   switch (n) {
 #define MFB_CASE(NN) case NN: flat_kernel<NN, MODE><<<grid, c.cta, c.smem, s>>>(a); break;
+    MFB_CASE(64) MFB_CASE(128) MFB_CASE(256) MFB_CASE(512) MFB_CASE(1024)
+    MFB_CASE(2048) MFB_CASE(4096) MFB_CASE(8192) MFB_CASE(16384)
+#undef MFB_CASE
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_rows(int n, const NConst &c, const FlatArgs &a, cudaStream_t s) {
+  switch (n) {
+#define MFB_CASE(NN) case NN: rows_kernel<NN><<<c.grid_rows, c.cta, c.smem, s>>>(a); break;
     MFB_CASE(64) MFB_CASE(128) MFB_CASE(256) MFB_CASE(512) MFB_CASE(1024)
     MFB_CASE(2048) MFB_CASE(4096) MFB_CASE(8192) MFB_CASE(16384)
 #undef MFB_CASE
@@ -578,7 +595,7 @@ static int run_rows_impl(mfb_plan *p, int d0, int nd, int t0, int nt, const int3
     return run_large(p, d0, nd, t0, nt, rows, cnt, binsize, threshold, start, end, nb, idx, val,
                      counts, rs);
   }
-  CUDA_TRY(launch_flat<MODE_PEAKS>((int)p->n, *p->c, a, p->stream));
+  CUDA_TRY(launch_rows((int)p->n, *p->c, a, p->stream));
   return MFB_OK;
 }
 
@@ -728,6 +745,22 @@ struct mfb_hplan {
   int32_t *prev_count = nullptr;
   const void *host_table = nullptr;
   long long host_rows = -1, host_nb = -1;
+  // mfb_hier_run_host with host data: the bins above the band are copied on
+  // a second stream while the coarse pass runs
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // mfb_hier_run_host repeated with identical arguments replays one CUDA
+  // graph of the whole run (captured on `cap` at the second such call)
+  struct RunKey {
+    int d0, nd, t0, nt, same;
+    uint32_t thr_bits, gate_bits;
+    size_t binsize, start, end;
+    const void *data, *records, *table, *info;
+  };
+  RunKey last_key, graph_key;
+  bool last_valid = false;
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t cap = nullptr;
 };
 
 extern "C" int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, size_t band,
@@ -759,6 +792,10 @@ extern "C" int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, 
     if (e == cudaSuccess) e = cudaMalloc(&h->prev_list, (size_t)ndata * ntmpl * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&h->prev_count, sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMemset(h->prev_count, 0, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMemset(h->trig_total, 0, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(h->ct, 0, (size_t)ntmpl * band * sizeof(float2));
     if (e == cudaSuccess) e = cudaMemset(h->fpow, 0, (size_t)ntmpl * sizeof(float));
@@ -789,6 +826,11 @@ extern "C" int mfb_hier_destroy(mfb_hplan *h) {
   cudaFree(h->trig_total);
   cudaFree(h->prev_list);
   cudaFree(h->prev_count);
+  if (h->side) cudaStreamDestroy(h->side);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->cap) cudaStreamDestroy(h->cap);
   free(h->tready);
   tc_coarse_destroy(h->tc);
   delete h;
@@ -897,7 +939,7 @@ __global__ void accumulate_triggers(const int32_t *count, unsigned long long *to
 static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t binsize,
                          float threshold, size_t start, size_t end, int64_t *idx, void *val,
                          int32_t *counts, int rs, int phase = 0, void *table = nullptr,
-                         long long *info = nullptr) {
+                         long long *info = nullptr, const void *data_host = nullptr) {
   if (!h) return fail(MFB_ERR_ARG, "null plan");
   mfb_plan *p = h->full;
   size_t nb;
@@ -911,6 +953,20 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
   int cs, ce;
   coarse_window(h, start, end, &cs, &ce);
   cudaStream_t s = p->stream;
+  bool join = false;
+  if (data_host && phase == 0) {
+    // all data rows from host memory: the band the coarse pass reads first,
+    // the rest on the side stream, joined before the refine
+    const size_t row = h->n * sizeof(float2), band = h->m * sizeof(float2);
+    CUDA_TRY(cudaMemcpy2DAsync(p->data, row, data_host, row, band, (size_t)h->nd,
+                               cudaMemcpyDefault, s));
+    CUDA_TRY(cudaEventRecord(h->ev_fork, s));
+    CUDA_TRY(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+    CUDA_TRY(cudaMemcpy2DAsync((char *)p->data + band, row, (const char *)data_host + band, row,
+                               row - band, (size_t)h->nd, cudaMemcpyDefault, h->side));
+    CUDA_TRY(cudaEventRecord(h->ev_join, h->side));
+    join = true;
+  }
   if (phase != 2) {
   CUDA_TRY(cudaMemsetAsync(h->fire_count, 0, sizeof(int32_t), s));
   if (counts) CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nd * nt * sizeof(int32_t), s));
@@ -954,6 +1010,7 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
   }
   }
   if (phase == 1) return MFB_OK;
+  if (join) CUDA_TRY(cudaStreamWaitEvent(s, h->ev_join, 0));
   // Refine the survivors with the full filter; no host decision in between.
   r = run_rows_impl(p, d0, nd, t0, nt, h->fire_list, h->fire_count, nd * nt, binsize, threshold,
                     start, end, idx, val, counts, rs);
@@ -1018,13 +1075,22 @@ extern "C" int mfb_hier_run_records(mfb_hplan *h, int d0, int nd, int t0, int nt
                        (char *)records + 8, counts, 2);
 }
 
+static uint32_t float_bits(float x) {
+  uint32_t u;
+  memcpy(&u, &x, sizeof u);
+  return u;
+}
+
 extern "C" int mfb_hier_run_host(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t binsize,
-                                 float threshold, size_t start, size_t end, void *records,
-                                 void *table, int64_t *info) {
+                                 float threshold, size_t start, size_t end, const void *data,
+                                 void *records, void *table, int64_t *info) {
   if (!h) return fail(MFB_ERR_ARG, "null plan");
   if (!records || !table) return fail(MFB_ERR_ARG, "null output");
   if (((uintptr_t)records | (uintptr_t)table) & 15)
     return fail(MFB_ERR_ARG, "records and table must be 16-byte aligned");
+  size_t nb;
+  int r = check_run(h->full, d0, nd, t0, nt, binsize, start, end, &nb);
+  if (r) return r;
   DeviceGuard dg(h->device);
   void *dtab = nullptr, *dinfo = nullptr;
   if (cudaHostGetDevicePointer(&dtab, table, 0) != cudaSuccess) {
@@ -1035,10 +1101,81 @@ extern "C" int mfb_hier_run_host(mfb_hplan *h, int d0, int nd, int t0, int nt, s
     cudaGetLastError();
     return fail(MFB_ERR_ARG, "info must be pinned (page-locked, mapped) host memory");
   }
-  int r = hier_run_impl(h, d0, nd, t0, nt, binsize, threshold, start, end, (int64_t *)records,
-                        (char *)records + 8, nullptr, 2, 0, dtab, (long long *)dinfo);
-  if (r) h->host_table = nullptr;
-  return r;
+  // A graph may hold copies from pinned host memory only (a pageable copy is
+  // synchronous and cannot be captured), and the two-pass large-n refine
+  // sizes its batches on the host.
+  bool graphable = !is_large(h->n);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(h->full->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    graphable = false;   // the caller is capturing: record the kernels into its graph
+  }
+  if (data) {
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, data) != cudaSuccess) {
+      cudaGetLastError();
+      graphable = false;
+    } else if (pa.type != cudaMemoryTypeHost) {
+      graphable = false;
+    }
+  }
+  mfb_hplan::RunKey key;
+  memset(&key, 0, sizeof key);
+  key.d0 = d0; key.nd = nd; key.t0 = t0; key.nt = nt;
+  key.same = dtab == h->host_table && (long long)nd * nt == h->host_rows &&
+             (long long)nb == h->host_nb;
+  key.thr_bits = float_bits(threshold);
+  key.gate_bits = float_bits(h->cal_thr);
+  key.binsize = binsize; key.start = start; key.end = end;
+  key.data = data; key.records = records; key.table = dtab; key.info = dinfo;
+  if (graphable && h->graph && memcmp(&key, &h->graph_key, sizeof key) == 0) {
+    CUDA_TRY(cudaGraphLaunch(h->graph, h->full->stream));
+    h->pairs += (long long)nd * nt;
+    return MFB_OK;
+  }
+  const bool repeat = h->last_valid && memcmp(&key, &h->last_key, sizeof key) == 0;
+  h->last_key = key;
+  h->last_valid = false;
+  if (graphable && repeat) {
+    // second call with these arguments: capture the run once, replay it after
+    // (the arguments equal the previous call's, so the host table is the
+    // one this plan wrote last: the captured run is the changed-rows one)
+    cudaStream_t user = h->full->stream;
+    const long long pairs0 = h->pairs;
+    h->full->stream = h->cap;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
+    int rc = MFB_OK;
+    cudaError_t e = cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      rc = hier_run_impl(h, d0, nd, t0, nt, binsize, threshold, start, end, (int64_t *)records,
+                         (char *)records + 8, nullptr, 2, 0, dtab, (long long *)dinfo, data);
+      e = cudaStreamEndCapture(h->cap, &g);
+    }
+    h->full->stream = user;
+    if (rc == MFB_OK && e == cudaSuccess && g) e = cudaGraphInstantiate(&x, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (rc == MFB_OK && e == cudaSuccess && x) {
+      if (h->graph) cudaGraphExecDestroy(h->graph);
+      h->graph = x;
+      h->graph_key = key;
+      CUDA_TRY(cudaGraphLaunch(x, user));
+      h->last_valid = true;
+      return MFB_OK;   // the captured call already counted its pairs
+    }
+    // capture failed: nothing ran; run the call directly
+    if (x) cudaGraphExecDestroy(x);
+    cudaGetLastError();
+    h->pairs = pairs0;
+  }
+  r = hier_run_impl(h, d0, nd, t0, nt, binsize, threshold, start, end, (int64_t *)records,
+                    (char *)records + 8, nullptr, 2, 0, dtab, (long long *)dinfo, data);
+  if (r) {
+    h->host_table = nullptr;
+    return r;
+  }
+  h->last_valid = true;
+  return MFB_OK;
 }
 
 extern "C" int mfb_hier_coarse_values(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t start,

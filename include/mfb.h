@@ -142,12 +142,17 @@ int mfb_hier_run_records(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t bi
    reset to empty, then the rows refined now are written.  Any other table is
    copied whole.  The caller must not write into the table between calls.
    info: pinned host int64[2] or NULL; receives the refined rows and the
-   bytes written into the table.  Read table and info after synchronising
-   the stream.  The plan's trigger total is updated as by mfb_hier_run.
+   bytes written into the table.  data: NULL, or all ndata data spectra
+   (ndata x n complex64) in host memory, copied into the plan's data rows
+   first -- the lowest band bins of every row ahead of the coarse pass, the
+   rest on a second stream while the coarse pass runs -- so the memory must
+   stay unchanged until the run has completed (pinned memory makes both
+   copies asynchronous).  Read table and info after synchronising the
+   stream.  The plan's trigger total is updated as by mfb_hier_run.
    Same contract as ap_hmf_run (src/hmf.c:222-328) for the table itself. */
 int mfb_hier_run_host(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t binsize,
-                      float threshold, size_t start, size_t end, void *records, void *table,
-                      int64_t *info);
+                      float threshold, size_t start, size_t end, const void *data,
+                      void *records, void *table, int64_t *info);
 /* mfb_hier_run split for measurement: phase 1 enqueues only the coarse pass
    and gate (dismissed rows written, survivor list built), phase 2 only the
    refine of the list phase 1 built; phase 0 is the whole run.  Lets a caller

@@ -128,7 +128,7 @@ def test_host_table_bytes_and_unpinned_table_rejected():
     pageable = np.empty(nd * nt * nb * 2 + 2, np.int64)
     ptr = (pageable.ctypes.data + 15) // 16 * 16
     L = _lib.lib()
-    rc = L.mfb_hier_run_host(hf._hplan, 0, nd, 0, nt, n // nb, 0.0, 0, n, rec.data_ptr(),
+    rc = L.mfb_hier_run_host(hf._hplan, 0, nd, 0, nt, n // nb, 0.0, 0, n, None, rec.data_ptr(),
                              ctypes.c_void_p(ptr), None)
     assert rc == -1 and b"pinned" in L.mfb_last_error()
 
@@ -158,3 +158,58 @@ def test_held_host_bank_then_row_update():
     hf.set_data(C.astype(np.complex128))         # converted: the filter holds its own copy
     out = hf.run(binsize=bs)
     assert not parity.compare(out["index"], out["value"], oracle.correlate(C, H), bs)
+
+
+def test_host_data_upload_overlapped_with_coarse_pass():
+    """A held host bank reaches the device inside the run call: the band
+    ahead of the coarse pass, the rest on a second stream joined before the
+    refine.  Every refined row must see the whole spectrum (gate 0: all)."""
+    import torch
+    n, nd, nt, band, bs = 4096, 5, 24, 512, 256
+    rng = np.random.default_rng(16)
+    H = noise(rng, (nt, n))
+    hf = _filter(n, nd, nt, band, "bf16x3", 0.0)
+    hf.set_templates(H)
+    for k in range(3):
+        D = noise(rng, (nd, n))
+        if k == 1:                                # pageable source, the same path
+            src = D
+        else:
+            pin = torch.empty((nd, n), dtype=torch.complex64, pin_memory=True)
+            pin.numpy()[:] = D
+            src = pin.numpy()
+        hf.set_data(src)
+        out = hf.run(binsize=bs)
+        assert not parity.compare(out["index"], out["value"], oracle.correlate(D, H), bs)
+        # a sub-block run after it reads the same uploaded rows
+        sub = hf.run(binsize=bs, data=(2, 3), templates=(4, 10))
+        assert not parity.compare(sub["index"], sub["value"],
+                                  oracle.correlate(D[2:5], H[4:14]), bs)
+
+
+def test_repeated_calls_replay_one_graph_with_fresh_inputs():
+    """Identical arguments from the third call on replay one captured graph
+    (upload, coarse pass, refine, table update); new contents of the same
+    pinned bank and other arguments in between must all come out right."""
+    import torch
+    n, nd, nt, band = 4096, 4, 32, 512
+    rng = np.random.default_rng(17)
+    H = noise(rng, (nt, n))
+    hf = _filter(n, nd, nt, band, "bf16x3", 0.0)
+    hf.set_templates(H)
+    hf.set_data(noise(rng, (nd, n)))
+    hf.set_coarse_threshold(float(np.quantile(hf.coarse_values(), 0.8)))
+    pin = torch.empty((nd, n), dtype=torch.complex64, pin_memory=True)
+    for k, bs in enumerate((256, 256, 256, 256, 512, 256, 256, 256)):
+        D = noise(rng, (nd, n))
+        pin.numpy()[:] = D
+        hf.set_data(pin.numpy())
+        out = hf.run(binsize=bs, threshold=300.0)
+        idx, val = _dense(hf, binsize=bs, threshold=300.0)
+        np.testing.assert_array_equal(out["index"], idx)
+        np.testing.assert_array_equal(out["value"], val)
+        hit = (out["index"] >= 0).any(-1)
+        assert not parity.compare(out["index"], out["value"], oracle.correlate(D, H), bs, 300.0,
+                                  rows_mask=hit)
+    pairs, _ = hf.stats
+    assert pairs == 16 * nd * nt                  # replays count their pairs once each
