@@ -11,6 +11,12 @@ that n, and keeps the fastest:
   {64, 128, 256} and 64 <= N1 <= 4096, i.e. which radix-16 transform sizes
   the two passes run, and so the column tile width 4096/N2 of the first pass.
 
+It also times the same probe job on its own launches (the kernels
+specialised for n, as one plan per job runs them) and records both costs per
+pair (``pp_us``, ``dedicated_pp_us``): ``batch.dedicated`` sends a job of
+that n to its own launches when the difference times its pairs exceeds the
+cost of a launch.
+
 Results are cached per (device name, n) for the process, and in a JSON file
 when ``MFB_TUNE_CACHE`` names one.
 """
@@ -81,17 +87,13 @@ def tune(n, device=None, reps=3, warmup=2):
     if stored is not None:
         _CACHE[key] = stored
         return dict(stored)
-    cands = candidates(n)
-    if len(cands) == 1:
-        _CACHE[key] = cands[0]
-        return dict(cands[0])
     nd, nt = probe_shape(n)
     tdev = torch.device("cuda", dev.index)
     g = torch.Generator(device=tdev).manual_seed(n)
     D = torch.randn(nd, n, dtype=torch.complex64, device=tdev, generator=g)
     H = torch.randn(nt, n, dtype=torch.complex64, device=tdev, generator=g)
-    best, best_ms = None, float("inf")
-    for cfg in cands:
+
+    def time_cfg(cfg):
         bf = BatchedFilter([Job(H, data=D, binsize=max(1, n // 16))], device=dev,
                            tune={n: cfg})
         for _ in range(warmup):
@@ -104,10 +106,18 @@ def tune(n, device=None, reps=3, warmup=2):
             bf.run()
         b.record()
         bf.wait()
-        ms = a.elapsed_time(b) / reps
         bf.close()
+        return a.elapsed_time(b) / reps
+
+    best, best_ms = None, float("inf")
+    for cfg in candidates(n):
+        ms = time_cfg(cfg)
         if ms < best_ms:
             best, best_ms = cfg, ms
+    best = dict(best)
+    pairs = nd * nt
+    best["pp_us"] = best_ms * 1e3 / pairs
+    best["dedicated_pp_us"] = time_cfg({"dedicated": True}) * 1e3 / pairs
     _CACHE[key] = best
     _store_file(key, best)
     return dict(best)

@@ -111,7 +111,9 @@ def test_autotuner_picks_a_valid_config():
     from apogee_b200.batch import BatchedFilter, Job
     for n in (2048, 32768):
         cfg = autotune.tune(n)
-        assert cfg in autotune.candidates(n)
+        kernel_cfg = {k: v for k, v in cfg.items() if k in ("split", "unit_items")}
+        assert kernel_cfg in autotune.candidates(n)
+        assert cfg["pp_us"] > 0 and cfg["dedicated_pp_us"] > 0
     rng = np.random.default_rng(5)
     n = 32768
     D, H = noise(rng, (2, n)), noise(rng, (3, n))
@@ -129,3 +131,38 @@ def test_plan_errors():
         BatchedFilter([Job(H, data=D, binsize=64)], tune={n: {"split": 256}})   # N1 = 32
     with pytest.raises(ValueError):
         Job(H, data=D, binsize=1)   # 8192 bins > 4096 for the four-step
+
+
+def test_own_launch_jobs_beside_the_persistent_launch():
+    """Jobs forced onto their own launches (single-CTA 8192/16384, two-pass
+    65536, a series job) next to persistent ones: same results, also replayed
+    from a graph."""
+    import torch
+    from apogee_b200.batch import BatchedFilter
+    jobs, refs = make_jobs(seed=2)
+    own_n = {8192, 16384, 65536, 1024}
+    tune = {n: {"dedicated": True} for n in own_n}
+    bf = BatchedFilter(jobs, tune=tune)
+    info = bf.info()
+    assert info["own_launch_jobs"] == sum(1 for j in jobs if j.n in own_n)
+    assert info["tickets"] > 0
+    bf.run()
+    bf.wait()
+    check(bf, refs)
+    bf.capture()
+    for r in bf._records:
+        r.fill_(7)
+    bf.replay()
+    torch.cuda.synchronize()
+    bf.wait()
+    check(bf, refs)
+    # every job on its own launches: no persistent launch at all
+    solo = BatchedFilter(jobs[:3], tune={j.n: {"dedicated": True} for j in jobs[:3]})
+    assert solo.info()["tickets"] == 0
+    solo.run()
+    solo.wait()
+    for i in range(3):
+        z, bs, thr, win = refs[i]
+        r = solo.result(i)
+        assert not parity.compare(r["index"], r["value"], z, bs, thr, win)
+

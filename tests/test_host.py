@@ -63,3 +63,17 @@ def test_no_cpu_fallback_without_device(monkeypatch):
     monkeypatch.setattr(device, "devices", lambda: [])
     with pytest.raises(RuntimeError):
         mf.MatchedFilter(4096, 1, 1)
+
+
+def test_batch_own_launch_rule():
+    """A job leaves the persistent launch when forced, or when its pairs times
+    the measured per-pair saving exceed the launch cost."""
+    from apogee_b200.batch import DEDICATED_LAUNCH_US, Job, dedicated
+    H = np.zeros((100, 4096), np.complex64)
+    D = np.zeros((10, 4096), np.complex64)
+    job = Job(H, data=D, binsize=256)              # 1000 pairs
+    assert not dedicated(job, {})
+    assert dedicated(job, {"dedicated": True})
+    gain = DEDICATED_LAUNCH_US / 1000.0
+    assert dedicated(job, {"pp_us": 0.02 + 2 * gain, "dedicated_pp_us": 0.02})
+    assert not dedicated(job, {"pp_us": 0.02 + 0.5 * gain, "dedicated_pp_us": 0.02})
