@@ -213,3 +213,31 @@ def test_repeated_calls_replay_one_graph_with_fresh_inputs():
                                   rows_mask=hit)
     pairs, _ = hf.stats
     assert pairs == 16 * nd * nt                  # replays count their pairs once each
+
+
+@pytest.mark.parametrize("n,band,coarse", [(4096, 512, "fp16x3"), (4096, 1024, "fp32"),
+                                           (65536, 4096, "fp32")])
+def test_host_table_other_kinds_and_lengths(n, band, coarse):
+    """The host-table run for the other coarse kinds and for the two-pass
+    large-n refine (no graph there: its batches are sized on the host)."""
+    import torch
+    nd, nt, bs = 3, 12, n // 16
+    rng = np.random.default_rng(n + band)
+    H = noise(rng, (nt, n))
+    hf = _filter(n, nd, nt, band, coarse, 0.0)
+    hf.set_templates(H)
+    hf.set_data(noise(rng, (nd, n)))
+    hf.set_coarse_threshold(float(np.quantile(hf.coarse_values(), 0.6)))
+    pin = torch.empty((nd, n), dtype=torch.complex64, pin_memory=True)
+    for _ in range(4):
+        D = noise(rng, (nd, n))
+        pin.numpy()[:] = D
+        hf.set_data(pin.numpy())
+        out = hf.run(binsize=bs, window=(n // 32, n - 7))
+        idx, val = _dense(hf, binsize=bs, window=(n // 32, n - 7))
+        np.testing.assert_array_equal(out["index"], idx)
+        np.testing.assert_array_equal(out["value"], val)
+        hit = (out["index"] >= 0).any(-1)
+        assert hit.any()
+        assert not parity.compare(out["index"], out["value"], oracle.correlate(D, H), bs, 0.0,
+                                  (n // 32, n - 7), rows_mask=hit)
