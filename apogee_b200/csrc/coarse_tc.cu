@@ -322,6 +322,9 @@ coarse_tc_ws_kernel(const TcKernelArgs a) {
   } else if (warp < 12) {
     // ---- stage-1 epilogue: quadrant q, pairs q (tile 0) and 4 + q (tile 1), f2 = lane
     const int q = warp & 3, f2 = lane;
+    float2 tw[16];                 // W512^(f2 j1), j1 = 0..15: the same for every item
+#pragma unroll
+    for (int j1 = 0; j1 < 16; j1++) tw[j1] = tw512[j1 * 32 + f2];
     int last = -1;
     for (int it = 0; it < nit; it++) {
       const int k = it % NSLOT;
@@ -343,7 +346,7 @@ coarse_tc_ws_kernel(const TcKernelArgs a) {
         for (int j1 = 0; j1 < 16; j1++) {
           const uint32_t *vv = s ? v1 : v0;
           const float yr = __uint_as_float(vv[2 * j1]), yi = __uint_as_float(vv[2 * j1 + 1]);
-          const float2 w = tw512[j1 * 32 + f2];
+          const float2 w = tw[j1];
           const float zr = fmaf(yr, w.x, -yi * w.y), zi = fmaf(yr, w.y, yi * w.x);
           uint32_t hi, lo;
           split2<FP16>(zr, zi, hi, lo);
