@@ -519,6 +519,9 @@ class HierarchicalFilter(MatchedFilter):
         self._hostdata = None  # host data bank, read by the device at run()
         self._upload_evt = None
         self._bound = None     # (plan, stream) last given to mfb_hier_set_stream
+        self._tver = 0         # template bank version (band selection cache)
+        self._band_sel = None  # (token, band) of the measured band selection
+        self.selection = None  # the last band selection: band, gates, measured costs
         self._outview = None   # (key, read-only PEAK_DTYPE view of the host table)
         torch = _torch()
         dev = torch.device("cuda", self.device.index)
@@ -624,24 +627,45 @@ class HierarchicalFilter(MatchedFilter):
                 a = torch.from_numpy(a)
             self._gt[index].copy_(a.reshape(-1))
         self._tdirty = True
+        self._tver += 1
         self._mark_ready("template", index)
 
     # ---- calibration -----------------------------------------------------------
     def _choose_band(self):
-        """Pinned band, else the widest decimation whose gate resolves."""
+        """Pinned band, else the band that runs fastest on this device among
+        those whose model gate resolves the budget (costmodel: the reference's
+        choose_config, python/matchedfilter/__init__.py:1040-1054, with costs
+        measured here on the caller's bank instead of read from a table)."""
         if self._pinned is not None:
             return self._pinned[0]
         if self._pending_ref is None:
             raise ValueError(
                 "no band: pin band= (and a coarse threshold) or set_reference() so the "
                 "gate model can place the threshold")
-        for band in (self.n // 8, self.n // 4, self.n // 2):
-            if band >= 64 and gatemodel.gate_for(self._pending_ref, self.n, band,
-                                                 self._fs_snr or self.snr, self.fd,
-                                                 device=self.device.index) is not None:
-                return band
-        raise ValueError("the gate model cannot resolve fd=%g at snr=%g for n=%d"
-                         % (self.fd, self.snr, self.n))
+        token = (id(self._pending_ref), self._tver, self._fs_snr or self.snr, self.fd)
+        if self._band_sel is not None and self._band_sel[0] == token:
+            return self._band_sel[1]
+        from . import costmodel
+        tc = self._kind != _lib.COARSE_FP32
+        gates = {}
+        for band in costmodel.candidate_bands(self.n, (lambda b: b == 512) if tc
+                                              else (lambda b: True)):
+            g = gatemodel.gate_for(self._pending_ref, self.n, band, self._fs_snr or self.snr,
+                                   self.fd, device=self.device.index)
+            if g is not None:
+                gates[band] = g
+        if not gates:
+            raise ValueError("the gate model cannot resolve fd=%g at snr=%g for n=%d"
+                             % (self.fd, self.snr, self.n))
+        if self._template_ready is not None:
+            band, costs = max(gates), {}          # no bank yet to measure with: widest
+        else:
+            band, costs = costmodel.choose(self, gates)
+            self._band_sel = (token, band)
+        self.selection = {"band": band, "gates": gates,
+                          "costs_us": {b: c[0] for b, c in costs.items()},
+                          "refine_rates": {b: c[1] for b, c in costs.items()}}
+        return band
 
     def _coarse_value(self, band):
         if self._cal_thr is not None:

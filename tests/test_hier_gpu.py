@@ -185,3 +185,37 @@ def test_tensor_core_coarse_tail_pairs():
     got = hf.coarse_values()
     want = oracle.coarse_max(D, H, band)
     assert np.abs(got - want).max() < 1e-4 * want.max()
+
+
+def test_band_selected_by_measured_cost():
+    """band=None with a reference: every candidate band whose gate resolves is
+    timed on the device with the caller's bank; the fastest is used, and the
+    result keeps the hierarchical contract (reported peaks are the flat
+    filter's)."""
+    mf = _mf()
+    n, nd, nt = 4096, 4, 64
+    rng = np.random.default_rng(21)
+    power = inspiral_power(n)
+    H = np.stack([template_with_power(n, power) for _ in range(nt)])
+    D = noise(rng, (nd, n))
+    D[1] += (12.0 * H[5] * np.exp(2j * np.pi * np.arange(n) * 777 / n)).astype(np.complex64)
+    hf = mf.HierarchicalFilter(n, nd, nt, snr=5.5, fd=1e-2, coarse="fp32")
+    hf.set_reference(power)
+    hf.set_templates(H)
+    hf.set_data(D)
+    b = hf.run(binsize=1024, threshold=5.5).copy()
+    sel = hf.selection
+    assert sel["band"] in sel["gates"] and sel["band"] == hf.config[0]
+    assert set(sel["costs_us"]) == set(sel["gates"])
+    if len(sel["gates"]) > 1:
+        assert sel["costs_us"][sel["band"]] == min(sel["costs_us"].values())
+    flat = mf.MatchedFilter(n, nd, nt)
+    flat.set_data(D)
+    flat.set_templates(H)
+    a = flat.run(binsize=1024, threshold=5.5)
+    fired = b["index"] >= 0
+    assert fired[1, 5].any()
+    np.testing.assert_array_equal(a["index"][fired], b["index"][fired])
+    # the choice is kept until the bank or the reference changes
+    hf.run(binsize=1024, threshold=5.5)
+    assert hf.selection is sel

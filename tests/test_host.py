@@ -77,3 +77,16 @@ def test_batch_own_launch_rule():
     gain = DEDICATED_LAUNCH_US / 1000.0
     assert dedicated(job, {"pp_us": 0.02 + 2 * gain, "dedicated_pp_us": 0.02})
     assert not dedicated(job, {"pp_us": 0.02 + 0.5 * gain, "dedicated_pp_us": 0.02})
+
+
+def test_costmodel_candidates_and_pick():
+    """Band candidates span n/16 .. n/2 (>= 64, as the kind allows); the
+    fastest measured band wins and ties go to the wider band."""
+    from apogee_b200 import costmodel
+    assert costmodel.candidate_bands(4096, lambda b: True) == [256, 512, 1024, 2048]
+    assert costmodel.candidate_bands(4096, lambda b: b == 512) == [512]
+    assert costmodel.candidate_bands(512, lambda b: True) == [64, 128, 256]
+    assert costmodel.pick({256: 40.0, 512: 31.0, 1024: 55.0}) == 512
+    assert costmodel.pick({256: 30.0, 512: 30.0}) == 512
+    with pytest.raises(ValueError):
+        costmodel.pick({})
