@@ -37,8 +37,28 @@ def candidates(n):
     return out
 
 
+#: What tune(n) found on a B200 (CUDA events, probe workload of probe_shape):
+#: the kernel configuration and the cost per pair (us) in the persistent launch
+#: and on the job's own launches.  Used when a batch is not tuned.
+B200 = {
+    1024: ({"unit_items": 8}, 0.0046, 0.0037),
+    2048: ({"unit_items": 8}, 0.0094, 0.0076),
+    4096: ({"unit_items": 8}, 0.0198, 0.0148),
+    8192: ({"split": 64}, 0.131, 0.038),
+    16384: ({"split": 64}, 0.235, 0.086),
+    32768: ({"split": 128}, 0.477, 0.335),
+    65536: ({"split": 256}, 0.940, 0.661),
+}
+
+
 def default(n):
-    """The configuration the library uses without tuning."""
+    """The configuration the library uses without tuning: the B200
+    measurement where there is one, else the kernel's own defaults."""
+    if n in B200:
+        cfg, pp, dp = B200[n]
+        out = dict(cfg)
+        out["pp_us"], out["dedicated_pp_us"] = pp, dp
+        return out
     if n <= 4096:
         return {"unit_items": 1}
     return {"split": 256 if n >= 16384 else 128}

@@ -133,8 +133,9 @@ class Job:
 class BatchedFilter:
     """Plan ``jobs`` for one persistent launch on a CUDA device.
 
-    tune : False (defaults), True (autotune every distinct n, cached per
-           device), or a dict {n: {"split": N2} | {"unit_items": k}}.
+    tune : False (``autotune.default``: the B200 measurements), True
+           (autotune every distinct n, cached per device), or a dict
+           {n: {"split": N2} | {"unit_items": k} | {"dedicated": True}}.
     slot_bytes, slots : scratch of the large-n four-step (0 = 64 MiB x 3).
     """
 
@@ -146,14 +147,14 @@ class BatchedFilter:
         self.jobs = list(jobs)
         if not self.jobs:
             raise ValueError("no jobs")
+        from . import autotune
         if tune is True:
-            from . import autotune
             self.config = {n: autotune.tune(n, device=self.device)
                            for n in sorted({j.n for j in self.jobs})}
         elif isinstance(tune, dict):
             self.config = dict(tune)
         else:
-            self.config = {}
+            self.config = {n: autotune.default(n) for n in sorted({j.n for j in self.jobs})}
         self._hold = []
         self._records = []
         self._plan = None
