@@ -491,8 +491,8 @@ class HierarchicalFilter(MatchedFilter):
             raise ValueError("ndata and ntemplates must be >= 1")
         if band is not None:
             band = int(band)
-            if band < 64 or band >= self.n or band & (band - 1):
-                raise ValueError("band must be a power of two, >= 64 and < n")
+            if band < 64 or band >= self.n or band & (band - 1) or band > 16384:
+                raise ValueError("band must be a power of two, >= 64, < n and <= 16384")
         if taps is not None:
             taps = int(taps)
             if taps < 2 or taps > 64 or taps % 2:
@@ -643,6 +643,8 @@ class HierarchicalFilter(MatchedFilter):
                 "no band: pin band= (and a coarse threshold) or set_reference() so the "
                 "gate model can place the threshold")
         token = (id(self._pending_ref), self._tver, self._fs_snr or self.snr, self.fd)
+        # (the data bank the costs were measured on is not part of the token: a
+        # choice made on one bank of the stream is kept for the next ones)
         if self._band_sel is not None and self._band_sel[0] == token:
             return self._band_sel[1]
         from . import costmodel
@@ -657,8 +659,8 @@ class HierarchicalFilter(MatchedFilter):
         if not gates:
             raise ValueError("the gate model cannot resolve fd=%g at snr=%g for n=%d"
                              % (self.fd, self.snr, self.n))
-        if self._template_ready is not None:
-            band, costs = max(gates), {}          # no bank yet to measure with: widest
+        if self._template_ready is not None or not self._dataset or self._data_ready is not None:
+            band, costs = max(gates), {}          # no bank or data yet to measure with: widest
         else:
             band, costs = costmodel.choose(self, gates)
             self._band_sel = (token, band)

@@ -7,15 +7,18 @@ requested budget, with costs read from tables measured on other machines
 machine").  Here the costs are measured on the device the filter runs on, at
 plan time, with the caller's own template bank:
 
-for every candidate band (a power of two, 64 <= band <= n/2, that the coarse
-kind supports) whose gate the model resolves, a plan at that band runs the
-whole hierarchical step -- coarse pass, gate at the model's threshold,
-refine of what passes -- on seeded noise data whose filter output has unit
-variance per component (the gate model's noise, gatemodel.gate_for), and
-CUDA events time it.  The fastest band wins; ties go to the wider band.
+for every candidate band (a power of two, 64 <= band <= min(n/2, 16384),
+that the coarse kind supports) whose gate the model resolves, a plan at that
+band runs the whole hierarchical step -- coarse pass, gate at the model's
+threshold, refine of what passes -- on the caller's own data bank, and CUDA
+events time it.  The refine rate, and so the cost, depends on the data as much
+as on the band (the model gate resolves the false-dismissal budget for signals
+at snr, not a noise rate), which is why the caller's data is used.  The
+fastest band wins; ties go to the wider band.
 
 Results are cached per (device, n, ndata, ntemplates, kind, snr, fd,
-reference, bank) for the process.
+reference, template bank) for the process: a choice measured on one data
+bank of a stream is kept for the next ones.
 """
 import hashlib
 
@@ -26,11 +29,14 @@ _CACHE = {}
 #: Timed repetitions per candidate (after one warm-up run).
 REPS = 3
 
+#: Widest coarse band: the coarse pass is the single-CTA filter at length band.
+MAX_BAND = 16384
+
 
 def candidate_bands(n, kind_supports_band):
     """Bands the reference's tables span at this n, narrowest first."""
     return [b for b in (n // 16, n // 8, n // 4, n // 2)
-            if b >= 64 and kind_supports_band(b)]
+            if 64 <= b <= MAX_BAND and kind_supports_band(b)]
 
 
 def pick(measured):
@@ -40,18 +46,6 @@ def pick(measured):
     if not measured:
         raise ValueError("no candidate band to choose from")
     return min(measured, key=lambda b: (measured[b], -b))
-
-
-def noise_bank(nd, n, energy, device, seed=20261204):
-    """(nd, n) complex64 noise spectra on `device` with per-bin variance
-    2 / energy, so that a template of that energy gives filter output with
-    unit variance in Re and Im."""
-    import torch
-    g = torch.Generator(device=device).manual_seed(seed)
-    scale = float(np.sqrt(1.0 / max(energy, 1e-30)))
-    re = torch.randn(nd, n, generator=g, device=device, dtype=torch.float32)
-    im = torch.randn(nd, n, generator=g, device=device, dtype=torch.float32)
-    return torch.complex(re * scale, im * scale)
 
 
 def _key(hf, candidates):
@@ -68,14 +62,13 @@ def _key(hf, candidates):
 def measure(hf, gates):
     """Microseconds of one hierarchical step per candidate band.
 
-    hf: the HierarchicalFilter being configured (templates set on the device);
+    hf: the HierarchicalFilter being configured (templates and data set);
     gates: {band: model gate}.  Returns {band: (us, refine_rate)}."""
     import torch
     from . import HierarchicalFilter
     kind = {v: k for k, v in _kinds().items()}[hf._kind]
     dev = torch.device("cuda", hf.device.index)
-    energy = float((hf._gt.abs() ** 2).sum(dim=1).mean().item())
-    D = noise_bank(hf.ndata, hf.n, energy, dev)
+    D = hf._gd if hf._hostdata is None else torch.from_numpy(hf._hostdata).to(dev)
     out = {}
     for band, gate in gates.items():
         p = HierarchicalFilter(hf.n, hf.ndata, hf.ntemplates, snr=hf.snr, fd=hf.fd, band=band,
