@@ -63,6 +63,7 @@ SIGNATURES = {
     "mfb_batch_create": (_I, [_PP, _I, ctypes.POINTER(MfbJob), _I, ctypes.POINTER(MfbBatchOpts)]),
     "mfb_batch_run": (_I, [_P, _P]),
     "mfb_batch_status": (_I, [_P, _P]),
+    "mfb_batch_test_wait_limit": (_I, [_P, _I]),
     "mfb_batch_info": (_I, [_P, _I64P, _IP, _IP, _IP, _SZP]),
     "mfb_batch_destroy": (_I, [_P]),
     "mfb_create": (_I, [_PP, _SZ, _I, _I, _I]),

@@ -1875,6 +1875,21 @@ extern "C" int mfb_batch_status(mfb_batch *b, void *stream) {
   return MFB_OK;
 }
 
+extern "C" int mfb_batch_test_wait_limit(mfb_batch *b, int delta) {
+  if (!b) return fail(MFB_ERR_ARG, "null batch");
+  if (b->nbatch < 1 || !b->args.a_total)
+    return fail(MFB_ERR_STATE, "the batch has no four-step pass to hold back");
+  if (delta != 1 && delta != -1) return fail(MFB_ERR_ARG, "delta must be +1 or -1");
+  DeviceGuard dg(b->device);
+  CUDA_TRY(cudaDeviceSynchronize());
+  unsigned *at = const_cast<unsigned *>(b->args.a_total);
+  unsigned v = 0;
+  CUDA_TRY(cudaMemcpy(&v, at, sizeof v, cudaMemcpyDeviceToHost));
+  v += (unsigned)delta;
+  CUDA_TRY(cudaMemcpy(at, &v, sizeof v, cudaMemcpyHostToDevice));
+  return MFB_OK;
+}
+
 extern "C" int mfb_batch_info(mfb_batch *b, int64_t *tickets, int *grid, int *segments,
                               int *batches, size_t *scratch_bytes) {
   if (!b) return fail(MFB_ERR_ARG, "null batch");

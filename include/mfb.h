@@ -230,6 +230,14 @@ int mfb_batch_run(mfb_batch *b, void *stream);
 /* Synchronises `stream`; MFB_ERR_CUDA if a dependency wait inside the last
    run ran out (the results of that run are then not valid). */
 int mfb_batch_status(mfb_batch *b, void *stream);
+/* Failure-detection test hook: adds delta (+1 or -1) to the pass-A unit
+   count that pass B of the first four-step batch waits for.  With +1 that
+   count is never reached: the next run's bounded dependency wait runs out
+   (a few seconds), the launch stops taking tickets and returns, and
+   mfb_batch_status reports MFB_ERR_CUDA; -1 restores the plan.  No GPU
+   fault, trap or hang is involved.  MFB_ERR_STATE if the batch has no
+   four-step pass.  Synchronous. */
+int mfb_batch_test_wait_limit(mfb_batch *b, int delta);
 /* Tickets, grid, segments, scratch batches and scratch bytes of the plan. */
 int mfb_batch_info(mfb_batch *b, int64_t *tickets, int *grid, int *segments, int *batches,
                    size_t *scratch_bytes);

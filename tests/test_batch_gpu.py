@@ -166,3 +166,33 @@ def test_own_launch_jobs_beside_the_persistent_launch():
         r = solo.result(i)
         assert not parity.compare(r["index"], r["value"], z, bs, thr, win)
 
+
+
+def test_dependency_wait_runs_out_and_is_reported():
+    """Failure detection without a GPU fault: pass B of the first four-step
+    batch is made to wait for a pass-A unit that never comes.  The bounded
+    wait runs out, the launch stops and returns, wait() raises, and the same
+    plan runs correctly once restored."""
+    import time
+    from apogee_b200 import _lib
+    from apogee_b200.batch import BatchedFilter, Job
+    rng = np.random.default_rng(31)
+    n = 32768
+    D, H = noise(rng, (2, n)), noise(rng, (3, n))
+    d2, h2 = noise(rng, (2, 1024)), noise(rng, (5, 1024))
+    bf = BatchedFilter([Job(H, data=D, binsize=1024), Job(h2, data=d2, binsize=64)],
+                       tune={n: {"split": 128}, 1024: {"unit_items": 2}})
+    L = _lib.lib()
+    _lib.check(L.mfb_batch_test_wait_limit(bf._plan, 1))
+    t0 = time.perf_counter()
+    bf.run()
+    with pytest.raises(RuntimeError, match="dependency wait ran out"):
+        bf.wait()
+    assert time.perf_counter() - t0 < 60
+    _lib.check(L.mfb_batch_test_wait_limit(bf._plan, -1))
+    bf.run()
+    bf.wait()
+    r = bf.result(0)
+    assert not parity.compare(r["index"], r["value"], oracle.correlate(D, H), 1024)
+    r = bf.result(1)
+    assert not parity.compare(r["index"], r["value"], oracle.correlate(d2, h2), 64)
