@@ -405,7 +405,7 @@ def our_arm(args):
 
     # end to end through the public API (host buffers both ways)
     # the step's input lives in pinned host memory; the result comes back as
-    # the refined rows of the table (the packed transfer of run())
+    # the rows of the table that changed (the host-table transfer of run())
     D_pin = torch.empty(D.shape, dtype=torch.complex64, pin_memory=True)
     D_pin.numpy()[:] = D
     D_host = D_pin.numpy()

@@ -28,7 +28,7 @@ def _dense(hf, **kw):
 
 
 @pytest.mark.parametrize("coarse", ["fp32", "bf16x3"])
-def test_packed_equals_dense_over_changing_survivors(coarse):
+def test_host_table_equals_dense_over_changing_survivors(coarse):
     n, nd, nt, band, bs, thr = 4096, 4, 64, 512, 256, 330.0
     rng = np.random.default_rng(11)
     H = noise(rng, (nt, n))
@@ -55,7 +55,7 @@ def test_packed_equals_dense_over_changing_survivors(coarse):
     assert len(seen) > 1                          # the survivor sets really changed
 
 
-def test_packed_gate_extremes_and_shape_changes():
+def test_host_table_gate_extremes_and_shape_changes():
     n, nd, nt, band = 4096, 3, 40, 512
     rng = np.random.default_rng(12)
     H = noise(rng, (nt, n))
@@ -91,7 +91,7 @@ def test_packed_gate_extremes_and_shape_changes():
     assert not parity.compare(d["index"], d["value"], z, 256, 0.0)
 
 
-def test_packed_result_is_read_only():
+def test_host_table_result_is_read_only():
     n, nd, nt = 4096, 2, 8
     rng = np.random.default_rng(13)
     hf = _filter(n, nd, nt, 512, "fp32", 0.0)
