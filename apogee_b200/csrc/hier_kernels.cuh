@@ -75,48 +75,92 @@ inline cudaError_t launch_hier_scale(const HierScaleArgs &a, cudaStream_t s) {
 // table (mapped memory, stores over the host link).  Every row the gate
 // dismisses is all empty records (index -1, value 0), so when the host table
 // holds the previous run's result only the rows that change cross the link:
-// the rows refined last time go back to empty (unwrite), then the rows
-// refined now are copied from the device table (write), in that stream order.
+// the rows refined now are written, and the rows refined last time but not
+// now are reset to empty.  Two launches in stream order:
+//   hier_write_kernel    writes the rows of this run's list and marks them
+//                        (bit p of mark[row], p the run's parity);
+//   hier_unwrite_kernel  resets the rows of the previous list that carry no
+//                        mark of this run, clears the previous run's mark bit,
+//                        stores this run's list for the next one (list store
+//                        p) and, in its last block, flips the parity.
+// State on the device (so that a CUDA graph of the run replays correctly):
+// mark[rows], list_store[2][rows], count_store[2], ctl = {parity, blocks
+// done, rows reset}.
 struct HierHostArgs {
   const int4 *records;        // device table [rows][nb]
   int4 *table;                // host table [rows][nb] (device-visible pointer)
   long long nb;
   const int32_t *list, *count;        // this run's refined rows
-  int32_t *prev_list, *prev_count;    // the rows the host table holds, updated here
+  uint32_t *mark;             // [rows]
+  int32_t *list_store;        // [2][rows]
+  int32_t *count_store;       // [2]
+  unsigned *ctl;              // [3]
+  long long rows;
   unsigned long long *total;  // plan's trigger total
   long long *info;            // host [2] (device-visible) or null: refined rows, bytes written
   int write_rows;             // 0: the table was copied whole, only bookkeeping
   long long full_bytes;       // bytes of that whole copy
 };
 
-static __global__ void hier_unwrite_kernel(const HierHostArgs a) {
-  const long long c = *a.prev_count;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  const int4 empty = make_int4(-1, -1, 0, 0);
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < c * a.nb; e += stride) {
-    const long long i = e / a.nb;
-    a.table[(long long)a.prev_list[i] * a.nb + (e - i * a.nb)] = empty;
-  }
-}
-
 static __global__ void hier_write_kernel(const HierHostArgs a) {
   const long long c = *a.count;
+  const uint32_t bit = 1u << (a.ctl[0] & 1u);
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (long long i = t0; i < c; i += stride) a.mark[a.list[i]] |= bit;   // rows are unique
   if (a.write_rows)
     for (long long e = t0; e < c * a.nb; e += stride) {
       const long long i = e / a.nb;
       const long long at = (long long)a.list[i] * a.nb + (e - i * a.nb);
       a.table[at] = a.records[at];
     }
-  for (long long i = t0; i < c; i += stride) a.prev_list[i] = a.list[i];
-  if (t0 == 0) {
-    const long long pc = *a.prev_count;
-    *a.total += (unsigned long long)c;
-    *a.prev_count = (int32_t)c;
-    if (a.info) {
-      a.info[0] = c;
-      a.info[1] = a.write_rows ? (pc + c) * a.nb * 16 : a.full_bytes;
+}
+
+static __global__ void hier_unwrite_kernel(const HierHostArgs a) {
+  const unsigned p = a.ctl[0] & 1u, q = p ^ 1u;
+  const uint32_t now = 1u << p, old = 1u << q;
+  const long long c = *a.count;
+  const long long pc = a.count_store[q];
+  const int32_t *prev = a.list_store + q * a.rows;
+  int32_t *keep = a.list_store + p * a.rows;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int4 empty = make_int4(-1, -1, 0, 0);
+  unsigned reset = 0;
+  if (a.write_rows)
+    for (long long e = t0; e < pc * a.nb; e += stride) {
+      const long long i = e / a.nb, j = e - i * a.nb;
+      const int32_t r = prev[i];
+      if (!(a.mark[r] & now)) {
+        a.table[(long long)r * a.nb + j] = empty;
+        if (j == 0) reset++;
+      }
+    }
+  __syncthreads();     // every thread of the block has read the marks it needs
+  for (long long i = t0; i < pc; i += stride) {
+    // the previous run's bit goes; a row refined again keeps this run's bit
+    // (its stale check above only reads `now`), the grid's other blocks read
+    // only rows of the previous list, each owned by one (i) here
+    atomicAnd(a.mark + prev[i], ~old);
+  }
+  for (long long i = t0; i < c; i += stride) keep[i] = a.list[i];
+  if (reset) atomicAdd(a.ctl + 2, reset);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(a.ctl + 1, 1u) == gridDim.x - 1) {     // last block of the grid
+      __threadfence();
+      const unsigned rs = atomicAdd(a.ctl + 2, 0u);
+      a.count_store[p] = (int32_t)c;
+      *a.total += (unsigned long long)c;
+      if (a.info) {
+        a.info[0] = c;
+        a.info[1] = a.write_rows ? ((long long)rs + c) * a.nb * 16 : a.full_bytes;
+      }
+      a.ctl[2] = 0;
+      a.ctl[1] = 0;
+      __threadfence();
+      a.ctl[0] = q;                                    // the next run's parity
     }
   }
 }

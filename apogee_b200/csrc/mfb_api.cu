@@ -740,9 +740,12 @@ struct mfb_hplan {
   unsigned long long *trig_total = nullptr;  // device: survivors summed over runs
   long long pairs = 0;
   TcCoarse *tc = nullptr;       // tensor-core coarse state
-  // mfb_hier_run_host: the rows refined in the host table it last wrote
-  int32_t *prev_list = nullptr; // [nd*nt]
-  int32_t *prev_count = nullptr;
+  // mfb_hier_run_host: which rows of the host table it last wrote hold refined
+  // rows (marks, the last two lists, run parity; see hier_kernels.cuh)
+  uint32_t *mark = nullptr;     // [nd*nt]
+  int32_t *list_store = nullptr;// [2][nd*nt]
+  int32_t *count_store = nullptr;
+  unsigned *ctl = nullptr;
   const void *host_table = nullptr;
   long long host_rows = -1, host_nb = -1;
   // mfb_hier_run_host with host data: the bins above the band are copied on
@@ -789,9 +792,14 @@ extern "C" int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, 
     if (e == cudaSuccess) e = cudaMalloc(&h->fire_list, (size_t)ndata * ntmpl * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&h->fire_count, sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&h->trig_total, sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMalloc(&h->prev_list, (size_t)ndata * ntmpl * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&h->prev_count, sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMemset(h->prev_count, 0, sizeof(int32_t));
+    const size_t rows = (size_t)ndata * ntmpl;
+    if (e == cudaSuccess) e = cudaMalloc(&h->mark, rows * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(h->mark, 0, rows * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&h->list_store, 2 * rows * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&h->count_store, 2 * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(h->count_store, 0, 2 * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&h->ctl, 3 * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(h->ctl, 0, 3 * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
@@ -824,8 +832,10 @@ extern "C" int mfb_hier_destroy(mfb_hplan *h) {
   cudaFree(h->fire_list);
   cudaFree(h->fire_count);
   cudaFree(h->trig_total);
-  cudaFree(h->prev_list);
-  cudaFree(h->prev_count);
+  cudaFree(h->mark);
+  cudaFree(h->list_store);
+  cudaFree(h->count_store);
+  cudaFree(h->ctl);
   if (h->side) cudaStreamDestroy(h->side);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
@@ -1024,8 +1034,11 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
     ha.nb = (long long)nb;
     ha.list = h->fire_list;
     ha.count = h->fire_count;
-    ha.prev_list = h->prev_list;
-    ha.prev_count = h->prev_count;
+    ha.mark = h->mark;
+    ha.list_store = h->list_store;
+    ha.count_store = h->count_store;
+    ha.ctl = h->ctl;
+    ha.rows = (long long)h->nd * h->nt;
     ha.total = h->trig_total;
     ha.info = info;
     ha.full_bytes = rows * (long long)nb * 16;
@@ -1034,13 +1047,12 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
     int sms = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
     const int grid = hier_host_grid(rows * (long long)nb, sms);
-    if (same) {
-      hier_unwrite_kernel<<<grid, 256, 0, s>>>(ha);
-      CUDA_TRY(cudaGetLastError());
-    } else {
-      CUDA_TRY(cudaMemcpyAsync(table, idx, (size_t)ha.full_bytes, cudaMemcpyDefault, s));
-    }
+    if (!same) CUDA_TRY(cudaMemcpyAsync(table, idx, (size_t)ha.full_bytes, cudaMemcpyDefault, s));
+    // this run's rows (and their marks), then the previous run's rows that
+    // no longer hold a refined row
     hier_write_kernel<<<grid, 256, 0, s>>>(ha);
+    CUDA_TRY(cudaGetLastError());
+    hier_unwrite_kernel<<<grid, 256, 0, s>>>(ha);
     CUDA_TRY(cudaGetLastError());
     h->host_table = table;
     h->host_rows = rows;

@@ -138,9 +138,9 @@ int mfb_hier_run_records(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t bi
    nd*nt*nb records, written by the device on the plan's stream.  Every row
    the gate dismisses is all empty records (index -1, value 0), so when
    `table` is the one this plan wrote last with the same nd*nt and nb, only
-   the rows that change cross the host link: the rows refined last time are
-   reset to empty, then the rows refined now are written.  Any other table is
-   copied whole.  The caller must not write into the table between calls.
+   the rows that change cross the host link: the rows refined now are
+   written, and the rows refined last time but not now are reset to empty.
+   Any other table is copied whole.  The caller must not write into the table between calls.
    info: pinned host int64[2] or NULL; receives the refined rows and the
    bytes written into the table.  data: NULL, or all ndata data spectra
    (ndata x n complex64) in host memory, copied into the plan's data rows

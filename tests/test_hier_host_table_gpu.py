@@ -116,7 +116,7 @@ def test_host_table_bytes_and_unpinned_table_rejected():
     full = nd * nt * nb * 16
     assert hf.last_d2h_bytes == full              # a new table is copied whole
     hf.run(binsize=n // nb)
-    assert hf.last_d2h_bytes == 2 * full          # every row reset, then written again
+    assert hf.last_d2h_bytes == full              # the same rows again: each written once
     hf.set_coarse_threshold(1e30)
     hf.run(binsize=n // nb)
     assert hf.last_d2h_bytes == full              # reset only
