@@ -358,6 +358,23 @@ class MatchedFilter:
         self._launch(None, idx, val, None, d0, nd, t0, nt, binsize, float(threshold), start, end)
         return idx.view(nd, nt, nb), val.view(nd, nt, nb)
 
+    def run_records(self, binsize=None, threshold=0.0, window=None, data=None, templates=None):
+        """run() without leaving the device, as one table of PEAK_DTYPE
+        records: a torch CUDA int64 tensor of shape (nd, nt, nb, 2) whose
+        bytes are the structured result (index, then the complex64 value's
+        bits), enqueued on torch's current stream and not synchronised.  A
+        host copy viewed as PEAK_DTYPE is what run() returns."""
+        torch = _torch()
+        binsize, start, end, d0, nd, t0, nt, nb = self._run_args(binsize, window, data, templates)
+        self._prepare_device()
+        rec = torch.empty(nd * nt * nb * 2, dtype=torch.int64,
+                          device=torch.device("cuda", self.device.index))
+        self._launch(rec, None, None, None, d0, nd, t0, nt, binsize, float(threshold), start, end)
+        return rec.view(nd, nt, nb, 2)
+
+    def _prepare_device(self):
+        self._bind_stream()
+
     # ---- series ---------------------------------------------------------------
     def _series_layout(self, series, starts, win_start, win_end, binsize, templates):
         from ._series import SeriesLayout
@@ -460,10 +477,20 @@ class MatchedFilter:
         self.clear_cache()
 
 
-def _coarse_kind(name):
+#: Bands the split-precision tensor-core coarse pass covers.
+TC_BANDS = frozenset([512])
+
+
+def _coarse_kind(name, band=None):
+    """Library coarse kind for `name` at `band` ("auto": the BF16 split
+    tensor-core pass where it covers the band, else the FP32 pass)."""
     kinds = {"bf16x3": _lib.COARSE_BF16X3, "fp16x3": _lib.COARSE_FP16X3, "fp32": _lib.COARSE_FP32}
+    if name == "auto":
+        if band is None:
+            return None
+        return _lib.COARSE_BF16X3 if band in TC_BANDS else _lib.COARSE_FP32
     if name not in kinds:
-        raise ValueError("coarse must be one of %s" % sorted(kinds))
+        raise ValueError("coarse must be one of %s" % sorted(list(kinds) + ["auto"]))
     return kinds[name]
 
 
@@ -478,12 +505,14 @@ class HierarchicalFilter(MatchedFilter):
     the reference profile by the gate model for (snr, fd).
 
     ``coarse`` picks the coarse arithmetic: ``"bf16x3"`` / ``"fp16x3"``
-    (split hi+lo tensor-core contraction, FP32 accumulation) or ``"fp32"``
-    (the flat FP32 kernel at length band, the reference's own method).
+    (split hi+lo tensor-core contraction, FP32 accumulation), ``"fp32"``
+    (the flat FP32 kernel at length band, the reference's own method), or
+    ``"auto"`` (default): the BF16 split tensor-core pass at the bands it
+    covers (TC_BANDS), the FP32 pass at the others.
     """
 
     def __init__(self, n, ndata=1, ntemplates=1, snr=5.5, fd=1e-2,
-                 band=None, taps=None, device=None, coarse="fp32"):
+                 band=None, taps=None, device=None, coarse="auto"):
         self.n = int(n)
         self.ndata = int(ndata)
         self.ntemplates = int(ntemplates)
@@ -502,7 +531,11 @@ class HierarchicalFilter(MatchedFilter):
             raise ValueError("device='gpu' supports n in %s; got %d" % (sorted(SIZES), self.n))
         self.snr = float(snr)
         self.fd = float(fd)
-        self._kind = _coarse_kind(coarse)
+        self._coarse = coarse
+        self._kind = _coarse_kind(coarse, band)
+        if self._kind not in (None, _lib.COARSE_FP32) and band is not None \
+                and band not in TC_BANDS:
+            raise ValueError("the %s coarse pass covers band in %s" % (coarse, sorted(TC_BANDS)))
         self._init_state()
         self._pinned = (band, int(taps or 8)) if band is not None else None
         self._pending_ref = None
@@ -553,6 +586,7 @@ class HierarchicalFilter(MatchedFilter):
             L.mfb_hier_destroy(self._hplan)
             self._hplan = None
         h = ctypes.c_void_p()
+        self._kind = _coarse_kind(self._coarse, band)
         _lib.check(L.mfb_hier_create(ctypes.byref(h), self.n, self.ndata, self.ntemplates,
                                      band, self._kind, self.device.index), "mfb_hier_create")
         self._hplan = h
@@ -648,9 +682,9 @@ class HierarchicalFilter(MatchedFilter):
         if self._band_sel is not None and self._band_sel[0] == token:
             return self._band_sel[1]
         from . import costmodel
-        tc = self._kind != _lib.COARSE_FP32
+        tc = self._coarse in ("bf16x3", "fp16x3")
         gates = {}
-        for band in costmodel.candidate_bands(self.n, (lambda b: b == 512) if tc
+        for band in costmodel.candidate_bands(self.n, (lambda b: b in TC_BANDS) if tc
                                               else (lambda b: True)):
             g = gatemodel.gate_for(self._pending_ref, self.n, band, self._fs_snr or self.snr,
                                    self.fd, device=self.device.index)
@@ -769,8 +803,7 @@ class HierarchicalFilter(MatchedFilter):
         k = min(int(templates), self.ntemplates)
         tsel = np.sort(rng.choice(self.ntemplates, size=k, replace=False))
         Hs = self._gt[tsel].cpu().numpy()
-        kind = {_lib.COARSE_FP32: "fp32", _lib.COARSE_BF16X3: "bf16x3",
-                _lib.COARSE_FP16X3: "fp16x3"}[self._kind]
+        kind = self._coarse
         chunk = 512
         kept = []
         flat = MatchedFilter(n, chunk, k, device=self.device)
@@ -883,6 +916,9 @@ class HierarchicalFilter(MatchedFilter):
             self._outview = (key, out, info.numpy())
         self.last_d2h_bytes = int(self._outview[2][1])
         return self._outview[1]
+
+    def _prepare_device(self):
+        self._prepare()
 
     def run_device(self, binsize=None, threshold=0.0, window=None, data=None, templates=None):
         torch = _torch()

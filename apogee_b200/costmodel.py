@@ -55,7 +55,7 @@ def _key(hf, candidates):
     # the bank enters through its size and a sample of rows (first, middle, last)
     for r in sorted({0, t.shape[0] // 2, t.shape[0] - 1}):
         h.update(t[r].cpu().numpy().tobytes())
-    return (hf.device.index, hf.n, hf.ndata, hf.ntemplates, hf._kind,
+    return (hf.device.index, hf.n, hf.ndata, hf.ntemplates, hf._coarse,
             hf._fs_snr or hf.snr, hf.fd, tuple(candidates), h.hexdigest())
 
 
@@ -66,7 +66,7 @@ def measure(hf, gates):
     gates: {band: model gate}.  Returns {band: (us, refine_rate)}."""
     import torch
     from . import HierarchicalFilter
-    kind = {v: k for k, v in _kinds().items()}[hf._kind]
+    kind = hf._coarse
     dev = torch.device("cuda", hf.device.index)
     D = hf._gd if hf._hostdata is None else torch.from_numpy(hf._hostdata).to(dev)
     out = {}
@@ -92,12 +92,6 @@ def measure(hf, gates):
         out[band] = (us, rate)
         del p
     return out
-
-
-def _kinds():
-    from . import _lib
-    return {"bf16x3": _lib.COARSE_BF16X3, "fp16x3": _lib.COARSE_FP16X3,
-            "fp32": _lib.COARSE_FP32}
 
 
 def choose(hf, gates):

@@ -847,6 +847,19 @@ extern "C" int mfb_hier_destroy(mfb_hplan *h) {
   return MFB_OK;
 }
 
+// Forget the captured run and the repeated-call record: the next
+// mfb_hier_run_host runs directly and captures again at the call after.
+// Every plan input goes through the setters below, so a replay never runs
+// with state that was changed after its capture.  (A graph still in flight
+// is released by CUDA when it completes.)
+static void hier_drop_graph(mfb_hplan *h) {
+  h->last_valid = false;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+}
+
 extern "C" int mfb_hier_set_stream(mfb_hplan *h, void *stream) {
   if (!h) return fail(MFB_ERR_ARG, "null plan");
   return mfb_set_stream(h->full, stream);
@@ -854,6 +867,7 @@ extern "C" int mfb_hier_set_stream(mfb_hplan *h, void *stream) {
 
 extern "C" int mfb_hier_set_data(mfb_hplan *h, int d0, int count, const void *spec) {
   if (!h) return fail(MFB_ERR_ARG, "null plan");
+  hier_drop_graph(h);
   return mfb_set_data(h->full, d0, count, spec);
 }
 
@@ -884,6 +898,7 @@ extern "C" int mfb_hier_set_templates(mfb_hplan *h, int t0, int count, const voi
   int r = mfb_set_templates(h->full, t0, count, spec);
   if (r) return r;
   DeviceGuard dg(h->device);
+  hier_drop_graph(h);
   HierFpowArgs f;
   f.tmpl = h->full->tmpl;
   f.n = (int)h->n;
@@ -899,6 +914,7 @@ extern "C" int mfb_hier_set_templates(mfb_hplan *h, int t0, int count, const voi
 extern "C" int mfb_hier_set_reference(mfb_hplan *h, const float *power) {
   if (!h) return fail(MFB_ERR_ARG, "null plan");
   DeviceGuard dg(h->device);
+  hier_drop_graph(h);
   if (power) {
     for (size_t k = 0; k < h->n; k++)
       if (!std::isfinite(power[k]) || power[k] < 0)
@@ -926,6 +942,10 @@ extern "C" int mfb_hier_set_reference(mfb_hplan *h, const float *power) {
 
 extern "C" int mfb_hier_set_threshold(mfb_hplan *h, float thr) {
   if (!h || !std::isfinite(thr)) return fail(MFB_ERR_ARG, "coarse threshold must be finite");
+  if (thr != h->cal_thr) {
+    DeviceGuard dg(h->device);
+    hier_drop_graph(h);
+  }
   h->cal_thr = thr;
   return MFB_OK;
 }

@@ -34,35 +34,47 @@ def _dist():
     return dist
 
 
-def all_gather_peaks(local, nt_total, group=None):
-    """Assemble the ``(nd, nt_total, nb)`` PEAK_DTYPE table from every rank's
-    ``(nd, count, nb)`` slice (its ``template_slice``).  ``local`` is a numpy
-    PEAK_DTYPE array; the exchange runs on the device of ``device`` below:
-    the rank's current CUDA device for NCCL groups, the CPU for gloo."""
+def all_gather_records(local, nt_total, group=None):
+    """Assemble the full ``(nd, nt_total, nb, 2)`` int64 record table (the
+    PEAK_DTYPE bytes: index, value bits) from every rank's ``(nd, count, nb,
+    2)`` slice, where the slice already lives: a CUDA tensor for NCCL groups
+    (one all-gather over NVLink, the table stays on the device, no host
+    copy), a CPU tensor for gloo.  Slices are padded to the largest one."""
     import torch
     dist = _dist()
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
+    if local.dtype != torch.int64 or local.dim() != 4 or local.shape[3] != 2:
+        raise TypeError("local must be an int64 (nd, count, nb, 2) record tensor")
+    nd, cnt, nb, _ = local.shape
+    want = template_slice(nt_total, rank, world)[1]
+    if cnt != want:
+        raise ValueError("rank %d holds %d templates; its slice has %d" % (rank, cnt, want))
+    maxc = template_slice(nt_total, 0, world)[1]
+    padded = local.new_zeros((nd, maxc, nb, 2))
+    padded[:, :cnt] = local
+    parts = [torch.empty_like(padded) for _ in range(world)]
+    dist.all_gather(parts, padded, group=group)
+    return torch.cat([parts[r][:, :template_slice(nt_total, r, world)[1]]
+                      for r in range(world)], dim=1)
+
+
+def all_gather_peaks(local, nt_total, group=None):
+    """all_gather_records for a numpy PEAK_DTYPE ``(nd, count, nb)`` slice
+    (a host result): the exchange runs on the rank's current CUDA device for
+    NCCL groups, on the CPU for gloo; returns the numpy table."""
+    import torch
+    dist = _dist()
     local = np.ascontiguousarray(local)
     if local.dtype != PEAK_DTYPE or local.ndim != 3:
         raise TypeError("local must be a (nd, count, nb) PEAK_DTYPE array")
     nd, cnt, nb = local.shape
-    t0, want = template_slice(nt_total, rank, world)
-    if cnt != want:
-        raise ValueError("rank %d holds %d templates; its slice has %d" % (rank, cnt, want))
-    maxc = template_slice(nt_total, 0, world)[1]
-    backend = dist.get_backend(group)
-    dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" \
-        else torch.device("cpu")
+    dev = torch.device("cuda", torch.cuda.current_device()) \
+        if dist.get_backend(group) == "nccl" else torch.device("cpu")
     if not local.flags.writeable:               # a hierarchical run's host table
         local = local.copy()
-    words = torch.from_numpy(local.view(np.int64).reshape(nd, cnt, nb * 2))
-    padded = torch.zeros(nd, maxc, nb * 2, dtype=torch.int64, device=dev)
-    padded[:, :cnt] = words.to(dev)
-    parts = [torch.empty_like(padded) for _ in range(world)]
-    dist.all_gather(parts, padded, group=group)
-    full = torch.cat([parts[r][:, :template_slice(nt_total, r, world)[1]]
-                      for r in range(world)], dim=1)
+    words = torch.from_numpy(local.view(np.int64).reshape(nd, cnt, nb, 2)).to(dev)
+    full = all_gather_records(words, nt_total, group)
     return full.cpu().numpy().view(PEAK_DTYPE).reshape(nd, nt_total, nb)
 
 
@@ -123,6 +135,12 @@ class ShardedFilter:
     def run(self, binsize=None, threshold=0.0, window=None):
         part = self.local.run(binsize=binsize, threshold=threshold, window=window)
         return all_gather_peaks(np.asarray(part), self.ntemplates, self.group)
+
+    def run_records(self, binsize=None, threshold=0.0, window=None):
+        """The full table as device records on every rank (NCCL): the rank's
+        slice from ``run_records`` of its filter, gathered in place."""
+        part = self.local.run_records(binsize=binsize, threshold=threshold, window=window)
+        return all_gather_records(part, self.ntemplates, self.group)
 
     @property
     def stats(self):

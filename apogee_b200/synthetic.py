@@ -88,12 +88,11 @@ def flat_workload(n=4096, nd=16, nt=1024, seed=0, n_injected=2, snr=8.0):
     return D.astype(np.complex64), H, inj
 
 
-def hier_workload(n=4096, nd=16, nt=1024, seed=1, frac=0.10, snr_lo=5.0, snr_hi=12.0):
-    """Hierarchical benchmark workload: noise data, `frac` of the segments
-    carry an injection at SNR U[snr_lo, snr_hi]; the reference profile is the
-    mean |h|^2 over the bank."""
-    rng = np.random.default_rng(seed)
-    H = template_bank(n, nt, rng)
+def hier_data(H, nd, rng, frac=0.10, snr_lo=5.0, snr_hi=12.0):
+    """Noise data for the bank H: `frac` of the nd segments (at least one)
+    carry a random template of H at a random lag and SNR U[snr_lo, snr_hi].
+    Returns (D complex64 [nd][n], injections [(d, t, lag, snr)])."""
+    nt, n = H.shape
     D = noise_spectra(n, nd, rng)
     k = max(1, int(round(frac * nd)))
     inj = []
@@ -102,8 +101,18 @@ def hier_workload(n=4096, nd=16, nt=1024, seed=1, frac=0.10, snr_lo=5.0, snr_hi=
         snr = float(rng.uniform(snr_lo, snr_hi))
         inject(D, H, d, t, lag, snr)
         inj.append((int(d), t, lag, snr))
+    return D.astype(np.complex64), inj
+
+
+def hier_workload(n=4096, nd=16, nt=1024, seed=1, frac=0.10, snr_lo=5.0, snr_hi=12.0):
+    """Hierarchical benchmark workload: noise data, `frac` of the segments
+    carry an injection at SNR U[snr_lo, snr_hi]; the reference profile is the
+    mean |h|^2 over the bank."""
+    rng = np.random.default_rng(seed)
+    H = template_bank(n, nt, rng)
+    D, inj = hier_data(H, nd, rng, frac, snr_lo, snr_hi)
     power = (np.abs(H.astype(np.complex128)) ** 2).mean(0).astype(np.float32)
-    return D.astype(np.complex64), H, power, inj
+    return D, H, power, inj
 
 
 def batched_workload(njobs=256, seed=2, device="cuda", nmin_log=10, nmax_log=16, nd_max=64,
@@ -150,3 +159,43 @@ def batched_workload(njobs=256, seed=2, device="cuda", nmin_log=10, nmax_log=16,
                          torch.exp(-2j * np.pi * k * lag / n)).to(torch.complex64)
             jobs.append(Job(H, data=D.to(torch.complex64).contiguous(), binsize=binsize))
     return jobs
+
+
+def large_workload(n=262144, nd=4, nt=2048, seed=1, device="cuda", frac=0.05, snr_lo=6.0,
+                   snr_hi=15.0, materialize=None, chunk=64):
+    """Large-transform bank: templates by the template_bank formula on bins
+    20..n/2-1, generated on the device; noise data (FFT(N(0,1))/sqrt(n)) with
+    `frac` of the segments (at least one) carrying a template at a random lag
+    and SNR U[snr_lo, snr_hi]; reference profile = mean |h|^2 over the bank.
+
+    materialize: None (every template) or a sequence of template indices to
+    return (a subsample of the same bank: the draws, the data and the profile
+    are those of the full bank).  Returns (D [nd][n] complex64, H [k][n]
+    complex64, power [n] float32, injections [(d, t, lag, snr)]) on `device`.
+    """
+    import torch
+    dev = torch.device(device)
+    rng = np.random.default_rng(seed)
+    alpha = torch.tensor(rng.uniform(1e2, 1e4, size=nt), dtype=torch.float64, device=dev)
+    tc = torch.tensor(rng.uniform(0, n, size=nt), dtype=torch.float64, device=dev)
+    rows = list(range(nt)) if materialize is None else [int(t) for t in materialize]
+    pos = {t: i for i, t in enumerate(rows)}
+    H = torch.empty(len(rows), n, dtype=torch.complex64, device=dev)
+    power = torch.zeros(n, dtype=torch.float64, device=dev)
+    for t0 in range(0, nt, chunk):
+        blk = template_bank_torch(n, alpha[t0:t0 + chunk], tc[t0:t0 + chunk]).to(torch.complex64)
+        power += (blk.abs().to(torch.float64) ** 2).sum(0)
+        for t in range(t0, min(t0 + chunk, nt)):
+            if t in pos:
+                H[pos[t]] = blk[t - t0]
+    power = (power / nt).to(torch.float32)
+    D = torch.from_numpy(noise_spectra(n, nd, rng)).to(dev)
+    k = torch.arange(n, device=dev, dtype=torch.float64)
+    inj = []
+    for d in rng.choice(nd, size=max(1, int(round(frac * nd))), replace=False):
+        t, lag, snr = int(rng.integers(nt)), int(rng.integers(n)), float(rng.uniform(snr_lo, snr_hi))
+        ht = template_bank_torch(n, alpha[t:t + 1], tc[t:t + 1])[0]
+        D[d] += snr * ht.to(torch.complex64).to(torch.complex128) * \
+            torch.exp(-2j * np.pi * k * lag / n)
+        inj.append((int(d), t, lag, snr))
+    return D.to(torch.complex64), H, power, inj

@@ -6,18 +6,24 @@ Workload (one GPU): n=4096, 16 data segments x 1024 templates = 16384 pairs,
 binsize 256 (16 bins), hierarchical band 512 (1/8), snr 5.5, fd 1e-2,
 threshold 5.5, reference profile = mean |h|^2 of the bank; synthetic seeded
 inputs (apogee_b200/synthetic.py), 10% of segments injected at SNR U[5,12].
-With --gpus N each rank filters its own 16 x 1024 block (its own template
-slice), so per-GPU work is fixed (weak scaling) and nothing is exchanged.
+Both arms use the same coarse threshold (CAL_GATE below); the gate model's
+own threshold is reported beside it.  With --gpus N each rank filters its own
+16 x 1024 block (its own template slice), so per-GPU work is fixed (weak
+scaling) and nothing is exchanged.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload hier|batched|large] [--no-sub]
 
 Prints ONE JSON line (rank 0).  `value` is device throughput with inputs
 resident in HBM, timed with CUDA events per step (L2 flushed between steps),
 max over ranks; `e2e` is the same metric through the public API
-(HierarchicalFilter.set_data from host memory + run() returning the numpy
-structured result).  `--impl reference` times the reference's own
-single-threaded CPU engine (built from its sources into oracle/_ref) on the
-same workload.
+(HierarchicalFilter.set_data from pinned host memory holding fresh data every
+step + run() returning the numpy structured result).  At one GPU the line also
+carries `configs`: the flat generator's workload, the adjoint, the n=262144
+bank and the batched jobs, each with its time and a parity summary.
+`--impl reference` times the reference's own CPU engine (built from its
+sources into oracle/_ref) on the same workload and gate, on every host thread,
+with the one-thread figure beside it.
 """
 import argparse
 import json
@@ -55,6 +61,15 @@ def measured_peaks():
         return 1590.0, 6650.0, "fallback (no MEASURED_PEAKS.json)"
 
 
+# Coarse threshold of the benchmark workload, shared by both arms: the
+# fd = 1e-2 quantile of the band-512 coarse maximum over pairs whose full
+# filter reaches snr 5.5, measured with FP64 correlations on 8192 independent
+# noise segments with injections (tests/golden/make_gate.py, which writes
+# tests/golden/gate_config1.json).  The gate model's own value for this
+# profile is reported beside it (model_gate).
+CAL_GATE = 3.7228326885529683
+GATE_DESC = ("fd=1e-2 quantile of the coarse maximum of detectable signals, FP64, "
+             "8192 independent noise segments (tests/golden/make_gate.py)")
 METRIC = "filter pairs/sec at n=4096: mixed-precision hier vs FP32 flat, same FD rate"
 WORKLOAD = ("hierarchical n=4096 ndata=16 ntemplates=1024 binsize=256 band=512 snr=5.5 "
             "fd=1e-2 threshold=5.5, 10% of segments injected at SNR U[5,12]")
@@ -74,7 +89,11 @@ def parse():
                          "jobs in one persistent launch; large: n=262144 bank, flat and "
                          "hierarchical")
     ap.add_argument("--jobs", type=int, default=256, help="batched workload: number of jobs")
+    ap.add_argument("--large-coarse", default="fp32", choices=["fp32", "bf16x3", "fp16x3"],
+                    help="large workload: coarse arithmetic of the hierarchical filter")
     ap.add_argument("--no-tune", action="store_true", help="batched workload: default configs")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="headline only: skip the per-configuration sub-records")
     return ap.parse_args()
 
 
@@ -167,8 +186,29 @@ class RefHierThreads:
         self.pool.shutdown()
 
 
+def workload_config():
+    """The `config` both arms print: workload, gate and pairs (identical)."""
+    return {"workload": WORKLOAD, "gate": GATE_DESC, "gate_value": CAL_GATE,
+            "pairs_per_gpu": ND * NT}
+
+
+def ref_single_thread(refcore, H, power, D, gate, seconds=2.0):
+    """The reference hierarchical engine as it runs by default: one plan on
+    one thread, warm run() calls over the whole 16 x 1024 workload."""
+    r = refcore.RefHier(N, ND, NT, BAND, gate, reference=power, snr=SNR, fd=FD)
+    r.set_templates(H)
+    r.set_data(D)
+    r.run(binsize=BINSIZE, threshold=THRESHOLD)
+    reps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds or reps < 3:
+        r.run(binsize=BINSIZE, threshold=THRESHOLD)
+        reps += 1
+    return reps * ND * NT / (time.perf_counter() - t0), reps
+
+
 def reference_arm(args):
-    """The reference's own CPU engine (oracle/_ref) on all host threads."""
+    """The reference's own CPU engine (oracle/_ref) on all host threads, at
+    the same gate as our arm; the one-thread figure beside it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -181,8 +221,7 @@ def reference_arm(args):
         return
     from apogee_b200 import synthetic, gatemodel
     D, H, power, _ = synthetic.hier_workload(N, ND, NT, seed=args.seed)
-    gate = gatemodel.gate_for(power, N, BAND, SNR, FD)
-    eng = RefHierThreads(refcore, H, power, gate, host_threads())
+    eng = RefHierThreads(refcore, H, power, CAL_GATE, host_threads())
     for _ in range(args.warmup):
         eng.step(D)
     t0 = time.perf_counter()
@@ -191,19 +230,32 @@ def reference_arm(args):
     dt = (time.perf_counter() - t0) / args.steps
     eng.close()
     v = ND * NT / dt
+    st_value, st_reps = ref_single_thread(refcore, H, power, D, CAL_GATE)
+    gate_model = gatemodel.gate_for(power, N, BAND, SNR, FD)
+    engm = RefHierThreads(refcore, H, power, gate_model, host_threads())
+    engm.step(D)
+    t0 = time.perf_counter()
+    for _ in range(max(3, args.steps // 4)):
+        engm.step(D)
+    model_v = max(3, args.steps // 4) * ND * NT / (time.perf_counter() - t0)
+    engm.close()
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "pairs/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD,
-                   "engine": "reference CPU engine, %d threads (one plan per thread over a "
-                             "template slice), HierarchicalFilter band=512 with the model gate"
-                             % eng.threads},
+        "config": workload_config(),
+        "engine": "reference CPU engine built from its sources, %d threads (one plan per "
+                  "thread over a template slice), HierarchicalFilter band=512" % eng.threads,
         "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": eng.threads,
                          "kind": "reference",
                          "sample": "the full 16x1024 workload per step, %d steps" % args.steps,
-                         "cpu": cpu_model(), "simd": refcore.core().backend()},
+                         "cpu": cpu_model(), "simd": refcore.core().backend(),
+                         "single_thread": {"value": st_value, "unit": "pairs/s", "cores": 1,
+                                           "sample": "one plan, %d warm runs of the full "
+                                                     "workload" % st_reps}},
+        "model_gate": {"gate_value": gate_model, "value": model_v, "unit": "pairs/s",
+                       "cores": eng.threads},
         "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -221,8 +273,9 @@ def cpu_model():
 
 # --------------------------------------------------------------- our arm
 def cpu_baseline_leg(D, H, power, gate, hier_idx):
-    """Rank 0, N=1: the reference CPU engine on a bounded sample, and the
-    false-dismissal of the device hierarchical result against FP64."""
+    """Rank 0, N=1: the reference CPU engine on a bounded sample at the
+    headline's gate (all host threads, and one thread), and the false
+    dismissal of each device hierarchical result against FP64."""
     out = {}
     try:
         from oracle import refcore, oracle
@@ -237,6 +290,7 @@ def cpu_baseline_leg(D, H, power, gate, hier_idx):
             reps += 1
         hier_v = reps * ND * NT / (time.perf_counter() - t0)
         eng.close()
+        st_value, st_reps = ref_single_thread(refcore, H, power, D, gate)
         f = refcore.RefFlat(N, ND, NT)
         f.set_templates(H)
         f.set_data(D)
@@ -244,9 +298,13 @@ def cpu_baseline_leg(D, H, power, gate, hier_idx):
         f.run(binsize=BINSIZE, threshold=THRESHOLD)
         flat_v = ND * NT / (time.perf_counter() - t0)
         out = {"value": hier_v, "unit": "pairs/s", "cores": eng.threads, "kind": "reference",
-               "sample": "full 16x1024 hierarchical workload, %d runs (~3 s), one plan per "
-                         "thread over a template slice; flat: 1 run on 1 thread" % reps,
-               "flat_value": flat_v, "cpu": cpu_model(), "simd": refcore.core().backend()}
+               "sample": "full 16x1024 hierarchical workload at the headline gate, %d runs "
+                         "(~3 s), one plan per thread over a template slice" % reps,
+               "single_thread": {"value": st_value, "unit": "pairs/s", "cores": 1,
+                                 "sample": "one plan, %d warm runs of the full workload"
+                                           % st_reps},
+               "flat_value": flat_v, "flat_sample": "flat filter, 1 run on 1 thread",
+               "cpu": cpu_model(), "simd": refcore.core().backend()}
     # false dismissal vs the FP64 flat filter, for each hierarchical result
     det = 0
     omit = {k: 0 for k in hier_idx}
@@ -263,6 +321,70 @@ def cpu_baseline_leg(D, H, power, gate, hier_idx):
     return out, fd
 
 
+def graph_of(dev, step, bind):
+    """One CUDA graph of `step` (after `bind`), warmed outside the capture."""
+    import torch
+    s = torch.cuda.Stream(dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(s):
+        bind()
+        step()
+    torch.cuda.current_stream(dev).wait_stream(s)
+    torch.cuda.synchronize(dev)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        bind()
+        step()
+    return g
+
+
+def timed_replays(dev, g, steps, warm, flush, world=1, sampler=None):
+    """Device milliseconds of `steps` replays of g (CUDA events per replay, L2
+    flushed before each, outside the events), max over ranks."""
+    import torch
+    import torch.distributed as dist
+    for _ in range(warm):
+        flush.zero_()
+        g.replay()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    if sampler:
+        # sustained load so that the clock samples see the GPU busy
+        sampler.start()
+        t_end = time.perf_counter() + 1.5
+        while time.perf_counter() < t_end:
+            for _ in range(50):
+                g.replay()
+            torch.cuda.synchronize(dev)
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        g.replay()
+        b.record()
+        evs.append((a, b))
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = sampler.stop() if sampler else None
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), clk
+
+
+def fp32_peak(local):
+    import ctypes
+    from apogee_b200 import _lib
+    peak = ctypes.c_double()
+    _lib.check(_lib.lib().mfb_fp32_peak(local, ctypes.byref(peak)))
+    return peak.value
+
+
 def our_arm(args):
     import torch
     import torch.distributed as dist
@@ -274,26 +396,25 @@ def our_arm(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    import ctypes
     import apogee_b200 as mf
     from apogee_b200 import synthetic, _lib
     dev = torch.device("cuda", local)
-    D, H, power, inj = synthetic.hier_workload(N, ND, NT, seed=args.seed + 1000 * rank)
+    seed = args.seed + 1000 * rank
+    D, H, power, inj = synthetic.hier_workload(N, ND, NT, seed=seed)
     gdev = "gpu:%d" % local
 
-    def make_hier(calibrated):
+    def make_hier(gate):
         hf = mf.HierarchicalFilter(N, ND, NT, snr=SNR, fd=FD, band=BAND, device=gdev,
                                    coarse=args.coarse)
         hf.set_reference(power)
         hf.set_templates(H)
-        if calibrated:
-            # independent noise and injections (its own seed), device filters only
-            hf.calibrate(snr=SNR, fd=FD, noise="real")
+        if gate is not None:
+            hf.set_coarse_threshold(gate)
         hf.set_data(D)
         return hf
 
-    hf_cal = make_hier(True)
-    hf_mod = make_hier(False)
+    hf_cal = make_hier(CAL_GATE)
+    hf_mod = make_hier(None)
     first_cal = hf_cal.run(binsize=BINSIZE, threshold=THRESHOLD).copy()
     first_mod = hf_mod.run(binsize=BINSIZE, threshold=THRESHOLD).copy()
     gate_model = hf_mod._coarse_value(BAND)
@@ -315,63 +436,15 @@ def our_arm(args):
         _lib.check(L.mfb_run(flat._plan, 0, ND, 0, NT, BINSIZE, THRESHOLD, 0, N,
                              idx.data_ptr(), val.data_ptr(), None))
 
-    def graph_of(step, bind):
-        s = torch.cuda.Stream(dev)
-        s.wait_stream(torch.cuda.current_stream(dev))
-        with torch.cuda.stream(s):
-            bind()
-            step()                                 # warm, outside capture
-        torch.cuda.current_stream(dev).wait_stream(s)
-        torch.cuda.synchronize(dev)
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            bind()
-            step()
-        return g
-
-    g_cal = graph_of(lambda: hier_step(hf_cal), hf_cal._bind_stream)
-    g_mod = graph_of(lambda: hier_step(hf_mod), hf_mod._bind_stream)
-    g_flat = graph_of(flat_step, flat._bind_stream)
-
-    def timed(g, steps, warm, sampler=None):
-        for _ in range(warm):
-            flush.zero_()
-            g.replay()
-        torch.cuda.synchronize(dev)
-        if world > 1:
-            dist.barrier()
-        if sampler:
-            # sustained load so that the clock samples see the GPU busy
-            sampler.start()
-            t_end = time.perf_counter() + 1.5
-            while time.perf_counter() < t_end:
-                for _ in range(50):
-                    g.replay()
-                torch.cuda.synchronize(dev)
-        evs = []
-        for _ in range(steps):
-            flush.zero_()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record()
-            g.replay()
-            b.record()
-            evs.append((a, b))
-        torch.cuda.synchronize(dev)
-        if world > 1:
-            dist.barrier()
-        clk = sampler.stop() if sampler else None
-        ms = sum(a.elapsed_time(b) for a, b in evs)
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item()), clk
+    g_cal = graph_of(dev, lambda: hier_step(hf_cal), hf_cal._bind_stream)
+    g_mod = graph_of(dev, lambda: hier_step(hf_mod), hf_mod._bind_stream)
+    g_flat = graph_of(dev, flat_step, flat._bind_stream)
 
     sampler = ClockSampler(local)
-    ms_cal, clocks = timed(g_cal, args.steps, args.warmup, sampler)
-    ms_mod, _ = timed(g_mod, args.steps, args.warmup)
+    ms_cal, clocks = timed_replays(dev, g_cal, args.steps, args.warmup, flush, world, sampler)
+    ms_mod, _ = timed_replays(dev, g_mod, args.steps, args.warmup, flush, world)
     flat_steps = max(3, args.steps // 2)
-    ms_flat, _ = timed(g_flat, flat_steps, args.warmup)
+    ms_flat, _ = timed_replays(dev, g_flat, flat_steps, args.warmup, flush, world)
     hier_ms_step = ms_cal / args.steps
     model_ms_step = ms_mod / args.steps
     flat_ms_step = ms_flat / flat_steps
@@ -403,36 +476,41 @@ def our_arm(args):
     phase_ms(hf_mod, 1, 1)
     trig_mod = hf_mod.last_refinements
 
-    # end to end through the public API (host buffers both ways)
-    # the step's input lives in pinned host memory; the result comes back as
-    # the rows of the table that changed (the host-table transfer of run())
+    # End to end through the public API (host buffers both ways), fresh data
+    # every step: banks of the same templates with new noise and injections,
+    # copied into the step's pinned input outside the timed region; the
+    # result comes back as the rows of the table that changed.
+    banks = [synthetic.hier_data(H, ND, np.random.default_rng(seed * 7919 + 17 + i))[0]
+             for i in range(8)]
     D_pin = torch.empty(D.shape, dtype=torch.complex64, pin_memory=True)
-    D_pin.numpy()[:] = D
     D_host = D_pin.numpy()
 
-    def e2e_step():
+    def e2e_step(i):
+        D_host[:] = banks[i % len(banks)]
+        t0 = time.perf_counter()
         hf_cal.set_data(D_host)
         hf_cal.run(binsize=BINSIZE, threshold=THRESHOLD)
-        return hf_cal.last_d2h_bytes
-    for _ in range(args.warmup):
-        e2e_step()
+        return time.perf_counter() - t0, hf_cal.last_d2h_bytes
+    for i in range(args.warmup):
+        e2e_step(i)
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
-    d2h_total = 0
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        d2h_total += e2e_step()
-    e2e_s = time.perf_counter() - t0
-    if not (hf_cal.run(binsize=BINSIZE, threshold=THRESHOLD) == first_cal).all():
-        raise RuntimeError("end-to-end table differs from the first run's")
+    e2e_s, d2h_total = 0.0, 0
+    for i in range(args.steps):
+        dt, nbytes = e2e_step(i)
+        e2e_s += dt
+        d2h_total += nbytes
+    last = hf_cal.run(binsize=BINSIZE, threshold=THRESHOLD).copy()
+    ridx, rval = hf_cal.run(raw=True, binsize=BINSIZE, threshold=THRESHOLD)
+    if not ((last["index"] == ridx).all() and (last["value"] == rval).all()):
+        raise RuntimeError("end-to-end table differs from the device table of the same data")
     t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * rows * args.steps / float(t.item())
 
-    peak = ctypes.c_double()
-    _lib.check(L.mfb_fp32_peak(local, ctypes.byref(peak)))
+    peak = fp32_peak(local)
     flat_flops = rows * FLOPS_PER_PAIR(N)
     flat_achieved = flat_flops / (flat_ms_step * 1e-3) / 1e12
     # coarse kernel: the reference's algorithmic flops of a band-point filter per pair
@@ -452,14 +530,15 @@ def our_arm(args):
             "flops_per_pair": TC_FLOPS_PER_PAIR,
             "hbm_frac": TRAFFIC_COARSE_TC / (coarse_ms * 1e-3) / (hbm_peak * 1e9),
             "fp32_equivalent": {"achieved": coarse_flops / (coarse_ms * 1e-3) / 1e12,
-                                "frac": coarse_flops / (coarse_ms * 1e-3) / peak.value,
+                                "frac": coarse_flops / (coarse_ms * 1e-3) / peak,
                                 "flops_per_pair": FLOPS_PER_PAIR(BAND)},
-            "peak_source": "bf16 dense GEMM " + peak_src + "; traffic from an ncu capture"}
+            "peak_source": "bf16 dense GEMM " + peak_src + " (of measured); traffic from an "
+                           "ncu capture"}
     else:
         roofline_line = {
             "bound": "fp32", "kernel": dominant,
-            "achieved": dom_flops / (dom_ms * 1e-3) / 1e12, "peak": peak.value / 1e12,
-            "unit": "TFLOP/s", "frac": dom_flops / (dom_ms * 1e-3) / peak.value,
+            "achieved": dom_flops / (dom_ms * 1e-3) / 1e12, "peak": peak / 1e12,
+            "unit": "TFLOP/s", "frac": dom_flops / (dom_ms * 1e-3) / peak,
             "traffic": TRAFFIC_FLAT if dominant == "refine" else None,
             "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak)"}
     if rank == 0:
@@ -469,11 +548,9 @@ def our_arm(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"fp32": "f32", "bf16x3": "bf16x3+f32", "fp16x3": "f16x3+f32"}[args.coarse],
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "coarse": args.coarse,
-                       "gate": "calibrated on the device at snr=5.5, fd=1e-2 from independent "
-                               "noise (HierarchicalFilter.calibrate)",
-                       "gate_value": hf_cal.calibration["gate"],
-                       "pairs_per_gpu": rows, "l2": "flushed (256 MiB write) between timed steps",
+            "config": workload_config(),
+            "method": {"coarse": args.coarse,
+                       "l2": "flushed (256 MiB write) between timed steps",
                        "timing": "CUDA events per step around a CUDA-graph replay"},
             "flat": {"value": flat_value, "unit": "pairs/s", "ms_per_step": flat_ms_step},
             "speedup_hier_vs_flat": value / flat_value,
@@ -481,34 +558,175 @@ def our_arm(args):
             "model_gate": {"gate_value": gate_model, "value": model_value,
                            "ms_per_step": model_ms_step, "refine_rate": trig_mod / rows,
                            "speedup_vs_flat": model_value / flat_value},
-            "kernels_ms": {"coarse_gate": coarse_ms, "refine": refine_ms},
+            "kernels_ms": {"coarse_gate": coarse_ms, "refine": refine_ms,
+                           "how": "each phase alone (mfb_hier_run_phase), CUDA events around "
+                                  "its launches, L2 flushed; the graph step overlaps their "
+                                  "launch latencies"},
             "roofline": roofline_line,
             "roofline_flat": {"bound": "fp32", "achieved": flat_achieved,
-                              "peak": peak.value / 1e12, "unit": "TFLOP/s",
-                              "frac": flat_achieved * 1e12 / peak.value,
+                              "peak": peak / 1e12, "unit": "TFLOP/s",
+                              "frac": flat_achieved * 1e12 / peak,
                               "flops_per_pair": FLOPS_PER_PAIR(N),
                               "traffic": TRAFFIC_FLAT,
                               "hbm_frac": TRAFFIC_FLAT / (flat_ms_step * 1e-3) / (hbm_peak * 1e9),
-                              "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak); "
-                                             "traffic from an ncu capture"},
+                              "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak, "
+                                             "of measured); %.1f TFLOP/s theoretical at the "
+                                             "median SM clock" % (
+                                                 148 * 128 * 2 * (clocks.get("sm_mhz") or 1965)
+                                                 * 1e6 / 1e12)},
             "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": ND * N * 8,
                     "d2h_bytes_per_step": d2h_total // args.steps,
                     "result": "full (%d, %d, %d) peak table on the host; the refined rows "
-                              "cross the link, every other row is empty" % (ND, NT, nb)},
+                              "cross the link, every other row is empty" % (ND, NT, nb),
+                    "data": "fresh every step: %d banks of the same templates with new noise "
+                            "and injections, copied into the pinned input outside the timed "
+                            "region" % len(banks)},
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
         }
         if world == 1:
-            cb, fd = cpu_baseline_leg(D, H, power, gate_model,
+            cb, fd = cpu_baseline_leg(D, H, power, CAL_GATE,
                                       {"calibrated": first_cal["index"],
                                        "model": first_mod["index"]})
             line["cpu_baseline"] = cb
             line["false_dismissal"] = fd
+    del g_cal, g_mod, g_flat, hf_cal, hf_mod, flat
+    if world == 1 and not args.no_sub:
+        torch.cuda.empty_cache()
+        line["configs"] = sub_records(args, dev, local, flush, peak)
+    if rank == 0:
         print(json.dumps(line))
-    del g_cal, g_mod, g_flat
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ------------------------------------------------- per-configuration records
+def sub_records(args, dev, local, flush, peak):
+    """The other benchmark configurations at one GPU, each with its time,
+    roofline and a parity or false-dismissal summary (a failure is reported
+    in its record and does not stop the others)."""
+    import torch
+    out = {}
+    for name, fn in (("config0_flat", sub_config0), ("config3_adjoint", sub_config3),
+                     ("config4_large", sub_config4), ("config2_batched", sub_config2)):
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn(args, dev, local, flush, peak)
+        except Exception as e:     # reported in the record
+            out[name] = {"error": "%s: %s" % (type(e).__name__, e)}
+        out[name]["wall_s"] = time.perf_counter() - t0
+        torch.cuda.synchronize(dev)
+        torch.cuda.empty_cache()
+    return out
+
+
+def sub_config0(args, dev, local, flush, peak):
+    """Flat FP32 filter on its own generator: n=4096, 16 x 1024, binsize 256,
+    threshold 0, 2 of 16 segments injected at SNR 8."""
+    import apogee_b200 as mf
+    from apogee_b200 import synthetic, _lib
+    import torch
+    D, H, inj = synthetic.flat_workload(N, ND, NT, seed=0)
+    f = mf.MatchedFilter(N, ND, NT, device="gpu:%d" % local)
+    f.set_data(D)
+    f.set_templates(H)
+    L = _lib.lib()
+    rows, nb = ND * NT, N // BINSIZE
+    rec = torch.empty(rows * nb * 2, dtype=torch.int64, device=dev)
+
+    def step():
+        _lib.check(L.mfb_run_records(f._plan, 0, ND, 0, NT, BINSIZE, 0.0, 0, N,
+                                     rec.data_ptr(), None))
+    g = graph_of(dev, step, f._bind_stream)
+    steps = max(5, args.steps // 2)
+    ms, _ = timed_replays(dev, g, steps, max(3, args.warmup), flush)
+    ms /= steps
+    out = f.run(binsize=BINSIZE, threshold=0.0).copy()
+    from oracle import oracle, parity
+    bad = parity.compare(out["index"][:, :128], out["value"][:, :128],
+                         oracle.correlate(D, H[:128]), BINSIZE, 0.0)
+    found = sum(int(abs(int(out["index"][d, t, lag // BINSIZE]) - lag) <= 8)
+                for d, t, lag, _ in inj)
+    flops = rows * FLOPS_PER_PAIR(N)
+    return {"workload": "flat n=4096 ndata=16 ntemplates=1024 binsize=256 threshold=0, 2 of 16 "
+                        "segments injected at SNR 8",
+            "value": rows / (ms * 1e-3), "unit": "pairs/s", "ms_per_step": ms,
+            "roofline": {"bound": "fp32", "achieved": flops / (ms * 1e-3) / 1e12,
+                         "peak": peak / 1e12, "unit": "TFLOP/s",
+                         "frac": flops / (ms * 1e-3) / peak, "traffic": TRAFFIC_FLAT,
+                         "peak_source": "measured FP32 FMA loop (mfb_fp32_peak), of measured"},
+            "parity": {"pairs_checked_fp64": ND * 128, "mismatches": len(bad),
+                       "injections_found": "%d/%d within 8 lags" % (found, len(inj))},
+            "timing": "CUDA events per CUDA-graph replay, L2 flushed, %d steps" % steps}
+
+
+def sub_config3(args, dev, local, flush, peak):
+    """Differentiable peak values: n=16384, 8 x 256, binsize 1024; forward +
+    backward of sum |peak|^2 through the adjoint kernel, and the gradient's
+    error against an FP64 torch.fft dense-correlation gradient."""
+    import torch
+    from apogee_b200 import synthetic
+    from apogee_b200.adjoint import peak_values
+    n, nd, nt, bs = 16384, 8, 256, 1024
+    rng = np.random.default_rng(3)
+    Hn = synthetic.template_bank(n, nt, rng)
+    Dn = synthetic.noise_spectra(n, nd, rng)
+    for d in range(0, nd, 3):
+        synthetic.inject(Dn, Hn, d, int(rng.integers(nt)), int(rng.integers(n)), 8.0)
+    D = torch.from_numpy(Dn.astype(np.complex64)).to(dev).requires_grad_(True)
+    H = torch.from_numpy(Hn).to(dev).requires_grad_(True)
+
+    def fwd_bwd():
+        D.grad = None
+        H.grad = None
+        _, _, power = peak_values(D, H, bs)
+        power.sum().backward()
+    for _ in range(3):
+        fwd_bwd()
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(max(5, args.steps // 4)):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        fwd_bwd()
+        b.record()
+        torch.cuda.synchronize(dev)
+        ms.append(a.elapsed_time(b))
+    idx, _, _ = peak_values(D, H, bs)
+    D64 = D.detach().to(torch.complex128).requires_grad_(True)
+    H64 = H.detach().to(torch.complex128).requires_grad_(True)
+    z = torch.fft.ifft(D64[:, None, :] * torch.conj(H64[None]), dim=-1) * n
+    zb = torch.gather(z, 2, idx.clamp(min=0))
+    ((zb.real ** 2 + zb.imag ** 2) * (idx >= 0)).sum().backward()
+    err = {}
+    for name, ours, ref in (("grad_data", D.grad, D64.grad), ("grad_templates", H.grad, H64.grad)):
+        ref = ref.resolve_conj()
+        diff = ours.to(torch.complex128) - ref
+        err[name] = {"rel_l2": (diff.norm() / ref.norm()).item(),
+                     "max_rel": (diff.abs().max() / ref.abs().max()).item()}
+    del z, zb
+    return {"workload": "adjoint n=16384 ndata=8 ntemplates=256 binsize=1024: forward + "
+                        "backward of sum |peak value|^2",
+            "ms_per_step": float(np.median(ms)), "unit": "ms",
+            "value": nd * nt / (float(np.median(ms)) * 1e-3), "value_unit": "pairs/s",
+            "gradient_vs_fp64_torch_fft": err,
+            "timing": "CUDA events around forward + backward, median of %d" % len(ms)}
+
+
+def sub_config4(args, dev, local, flush, peak):
+    rec = large_record(dev, local, args.seed, steps=3, warmup=2, coarse="fp32",
+                       cpu_sample=False)
+    rec.pop("clocks", None)
+    return rec
+
+
+def sub_config2(args, dev, local, flush, peak):
+    rec = batched_record(dev, local, args.seed, 256, steps=2, warmup=1, tune=False,
+                         peak=peak)
+    rec.pop("clocks", None)
+    return rec
 
 
 # ------------------------------------------------------- batched workload
@@ -571,43 +789,33 @@ def per_job_plans(jobs, dev_index):
     return total_ms
 
 
-def batched_arm(args):
-    import ctypes
+def batched_record(dev, local, seed, njobs, steps, warmup, tune, peak, world=1, rank=0):
+    """Time the config-2 generator's first `njobs` jobs in the batched engine
+    (one CUDA graph: the persistent launch plus the jobs' own launches)
+    against the same jobs one plan per job."""
     import torch
     import torch.distributed as dist
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    from apogee_b200 import synthetic, _lib, autotune
+    from apogee_b200 import synthetic, autotune
     from apogee_b200.batch import BatchedFilter
-    dev = torch.device("cuda", local)
     t0 = time.perf_counter()
-    jobs = synthetic.batched_workload(njobs=args.jobs, seed=args.seed + 1000 * rank,
-                                      device=str(dev))
+    jobs = synthetic.batched_workload(njobs=njobs, seed=seed + 1000 * rank, device=str(dev))
     torch.cuda.synchronize(dev)
     gen_s = time.perf_counter() - t0
     pairs = sum(j.pairs for j in jobs)
     flops = float(sum(j.pairs * FLOPS_PER_PAIR(j.n) for j in jobs))
     tmpl_bytes = sum(j.nt * j.n * 8 for j in jobs)
     t0 = time.perf_counter()
-    bf = BatchedFilter(jobs, device="gpu:%d" % local, tune=not args.no_tune)
+    bf = BatchedFilter(jobs, device="gpu:%d" % local, tune=tune)
     plan_s = time.perf_counter() - t0
     bf.capture()
-    for _ in range(max(args.warmup, 1)):
+    for _ in range(max(warmup, 1)):
         bf.replay()
     torch.cuda.synchronize(dev)
     bf.wait()
-    peak = ctypes.c_double()
-    _lib.check(_lib.lib().mfb_fp32_peak(local, ctypes.byref(peak)))
     sampler = ClockSampler(local)
     sampler.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
+          for _ in range(steps)]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -620,39 +828,59 @@ def batched_arm(args):
         dist.barrier()
     clocks = sampler.stop()
     bf.wait()
-    ms = [a.elapsed_time(b) for a, b in ev]
-    ms_step = float(np.mean(ms))
+    ms_step = float(np.mean([a.elapsed_time(b) for a, b in ev]))
     if world > 1:
         tmax = torch.tensor([ms_step], device=dev)
         dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
         ms_step = float(tmax.item())
-    base_ms = per_job_plans(jobs, local)
-    if rank == 0:
-        value = pairs * world / (ms_step * 1e-3)
-        print(json.dumps({
-            "metric": BATCH_METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded, generated on the device)",
-            "config": {"workload": BATCH_WORKLOAD % args.jobs, "pairs_per_gpu": pairs,
-                       "templates_gb": tmpl_bytes / 1e9, "tuned": autotune.tuned(),
-                       "plan": bf.info(), "generate_s": gen_s, "plan_s": plan_s,
-                       "l2": "inputs (%.0f GB) far larger than L2" % (tmpl_bytes / 1e9),
-                       "timing": "CUDA events around each CUDA-graph replay of the one launch"},
-            "per_job_plans": {"value": pairs / (base_ms * 1e-3), "unit": "pairs/s",
-                              "ms": base_ms,
-                              "how": "one mfb plan per job (mfb_run / mfb_run_series), "
-                                     "device time summed over jobs"},
-            "speedup_vs_per_job_plans": base_ms / ms_step,
-            "roofline": {"bound": "fp32", "achieved": flops / (ms_step * 1e-3) / 1e12,
-                         "peak": peak.value / 1e12, "unit": "TFLOP/s",
-                         "frac": flops / (ms_step * 1e-3) / peak.value, "traffic": None,
-                         "flops": "5 n log2 n + 9 n per pair, summed over jobs",
-                         "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak)"},
-            "gpu_launches": args.steps,
-            "clocks": clocks,
-        }))
+    info = bf.info()
     bf.close()
+    base_ms = per_job_plans(jobs, local)
+    return {
+        "workload": BATCH_WORKLOAD % njobs, "value": pairs * world / (ms_step * 1e-3),
+        "unit": "pairs/s", "ms_per_step": ms_step, "pairs_per_gpu": pairs,
+        "templates_gb": tmpl_bytes / 1e9, "tuned": autotune.tuned() if tune else False,
+        "plan": info, "generate_s": gen_s, "plan_s": plan_s,
+        "l2": "inputs (%.0f GB) far larger than L2" % (tmpl_bytes / 1e9),
+        "timing": "CUDA events around each CUDA-graph replay",
+        "per_job_plans": {"value": pairs / (base_ms * 1e-3), "unit": "pairs/s", "ms": base_ms,
+                          "how": "one mfb plan per job (mfb_run / mfb_run_series), "
+                                 "device time summed over jobs"},
+        "speedup_vs_per_job_plans": base_ms / ms_step,
+        "roofline": {"bound": "fp32", "achieved": flops / (ms_step * 1e-3) / 1e12,
+                     "peak": peak / 1e12, "unit": "TFLOP/s",
+                     "frac": flops / (ms_step * 1e-3) / peak, "traffic": None,
+                     "flops": "5 n log2 n + 9 n per pair, summed over jobs",
+                     "peak_source": "measured FP32 FMA loop on this GPU (mfb_fp32_peak)"},
+        "clocks": clocks,
+    }
+
+
+def batched_arm(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    peak = fp32_peak(local)
+    rec = batched_record(dev, local, args.seed, args.jobs, args.steps, args.warmup,
+                         not args.no_tune, peak, world, rank)
+    if rank == 0:
+        line = {"metric": BATCH_METRIC, "value": rec.pop("value"), "unit": "pairs/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": rec.pop("ms_per_step"), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded, generated on the device)",
+                "config": {"workload": rec.pop("workload")},
+                "gpu_launches": args.steps, "clocks": rec.pop("clocks")}
+        line.update(rec)
+        print(json.dumps(line))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -664,29 +892,8 @@ LSNR, LFD, LTHR = 6.0, 1e-3, 6.0
 LARGE_METRIC = "filter pairs/sec at n=262144: flat and hierarchical (band n/16, fd=1e-3)"
 LARGE_WORKLOAD = ("n=262144 ndata=4 ntemplates=2048 (4.3 GB of complex64 templates) binsize=4096; "
                   "templates by the config-0 formula on bins 20..n/2-1, data FFT(N(0,1))/sqrt(n), "
-                  "5%% of segments (at least one) injected at SNR U[6,15]; hierarchical band "
+                  "5% of segments (at least one) injected at SNR U[6,15]; hierarchical band "
                   "n/16 with the FP32 coarse pass, snr=6, fd=1e-3, threshold=6")
-
-
-def large_workload(dev, seed):
-    import torch
-    from apogee_b200 import synthetic
-    rng = np.random.default_rng(seed)
-    alpha = torch.tensor(rng.uniform(1e2, 1e4, size=LNT), dtype=torch.float64, device=dev)
-    tc = torch.tensor(rng.uniform(0, LN, size=LNT), dtype=torch.float64, device=dev)
-    H = torch.empty(LNT, LN, dtype=torch.complex64, device=dev)
-    for t0 in range(0, LNT, 64):
-        H[t0:t0 + 64] = synthetic.template_bank_torch(LN, alpha[t0:t0 + 64],
-                                                      tc[t0:t0 + 64]).to(torch.complex64)
-    D = torch.from_numpy(synthetic.noise_spectra(LN, LND, rng)).to(dev)
-    k = torch.arange(LN, device=dev, dtype=torch.float64)
-    inj = []
-    for d in rng.choice(LND, size=max(1, int(round(0.05 * LND))), replace=False):
-        t, lag, snr = int(rng.integers(LNT)), int(rng.integers(LN)), float(rng.uniform(6, 15))
-        D[d] += snr * H[t].to(torch.complex128) * torch.exp(-2j * np.pi * k * lag / LN)
-        inj.append((int(d), t, lag, snr))
-    power = (H.abs().to(torch.float64) ** 2).mean(0).to(torch.float32)
-    return D.to(torch.complex64), H, power, inj
 
 
 def fp64_detections(D, H, thr):
@@ -704,22 +911,20 @@ def fp64_detections(D, H, thr):
     return det
 
 
-def large_arm(args):
-    import ctypes
+def large_record(dev, local, seed, steps, warmup, coarse, cpu_sample=True, rank=0):
+    """Config 4: the n = 262144 bank, flat and hierarchical, with the false
+    dismissal of both against an FP64 dense correlation."""
     import torch
     import apogee_b200 as mf
-    from apogee_b200 import _lib
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank = int(os.environ.get("RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    D, H, power, inj = large_workload(dev, args.seed + 1000 * rank)
+    from apogee_b200 import synthetic
+    D, H, power, inj = synthetic.large_workload(LN, LND, LNT, seed=seed + 1000 * rank,
+                                                device=str(dev))
     gdev = "gpu:%d" % local
     flat = mf.MatchedFilter(LN, LND, LNT, device=gdev)
     flat.set_data(D)
     flat.set_templates(H)
     hf = mf.HierarchicalFilter(LN, LND, LNT, snr=LSNR, fd=LFD, band=LBAND, device=gdev,
-                               coarse="fp32")
+                               coarse=coarse)
     hf.set_reference(power.cpu().numpy())
     hf.set_templates(H)
     hf.set_data(D)
@@ -742,10 +947,9 @@ def large_arm(args):
 
     sampler = ClockSampler(local)
     sampler.start()
-    flat_ms = timed(lambda: flat.run_device(binsize=LBIN, threshold=LTHR), args.steps,
-                    max(args.warmup, 3))
-    hier_ms = timed(lambda: hf.run_device(binsize=LBIN, threshold=LTHR), args.steps,
-                    max(args.warmup, 3))
+    flat_ms = timed(lambda: flat.run_device(binsize=LBIN, threshold=LTHR), steps,
+                    max(warmup, 2))
+    hier_ms = timed(lambda: hf.run_device(binsize=LBIN, threshold=LTHR), steps, max(warmup, 2))
     clocks = sampler.stop()
     hidx, _ = hf.run_device(binsize=LBIN, threshold=LTHR)
     fidx, _ = flat.run_device(binsize=LBIN, threshold=LTHR)
@@ -754,11 +958,12 @@ def large_arm(args):
     missed_h = int((det & (hidx < 0)).sum().item())
     missed_f = int((det & (fidx < 0)).sum().item())
     refine = hf.refine_rate
-    peak = ctypes.c_double()
-    _lib.check(_lib.lib().mfb_fp32_peak(local, ctypes.byref(peak)))
+    gate = hf._coarse_value(LBAND)
+    del flat, hf
+    peak = fp32_peak(local)
     flops = FLOPS_PER_PAIR(LN) * pairs
     cb = None
-    if rank == 0:
+    if cpu_sample and rank == 0:
         try:
             from oracle import refcore
             if refcore.available():
@@ -777,30 +982,49 @@ def large_arm(args):
                                 "%d runs" % (k, reps), "cpu": cpu_model()}
         except Exception as e:   # reported, not fatal
             cb = {"unavailable": str(e)}
+    return {
+        "workload": LARGE_WORKLOAD.replace("FP32 coarse pass", {
+            "fp32": "FP32 coarse pass", "fp16x3": "FP16 split-precision tensor-core coarse "
+                                                  "pass", "bf16x3": "BF16 split-precision "
+                                                                    "tensor-core coarse pass"}[
+            coarse]),
+        "value": pairs / (hier_ms * 1e-3), "unit": "pairs/s", "ms_per_step": hier_ms,
+        "gate": gate,
+        "timing": "CUDA events per step, %d steps; the refine of the survivors reads their "
+                  "count on the host at this n" % steps,
+        "flat": {"value": pairs / (flat_ms * 1e-3), "unit": "pairs/s", "ms_per_step": flat_ms,
+                 "fp64_detections_missed": missed_f},
+        "hier": {"value": pairs / (hier_ms * 1e-3), "ms_per_step": hier_ms, "coarse": coarse,
+                 "refine_rate": refine, "speedup_vs_flat": flat_ms / hier_ms},
+        "false_dismissal": {"fp64_detections": n_det, "missed": missed_h,
+                            "rate": missed_h / n_det if n_det else 0.0, "injections": inj},
+        "roofline_flat": {"bound": "fp32", "achieved": flops / (flat_ms * 1e-3) / 1e12,
+                          "peak": peak / 1e12, "unit": "TFLOP/s",
+                          "frac": flops / (flat_ms * 1e-3) / peak,
+                          "flops_per_pair": FLOPS_PER_PAIR(LN),
+                          "peak_source": "measured FP32 FMA loop on this GPU, of measured"},
+        "cpu_baseline": cb,
+        "clocks": clocks,
+    }
+
+
+def large_arm(args):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    rec = large_record(dev, local, args.seed, args.steps, args.warmup, args.large_coarse,
+                       rank=rank)
     if rank == 0:
-        print(json.dumps({
-            "metric": LARGE_METRIC, "value": pairs / (hier_ms * 1e-3), "unit": "pairs/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": hier_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded, generated on the device)",
-            "config": {"workload": LARGE_WORKLOAD, "gate": hf._coarse_value(LBAND),
-                       "timing": "CUDA events per step; the refine of the survivors reads "
-                                 "their count on the host at this n"},
-            "flat": {"value": pairs / (flat_ms * 1e-3), "unit": "pairs/s", "ms_per_step": flat_ms,
-                     "fp64_detections_missed": missed_f},
-            "hier": {"value": pairs / (hier_ms * 1e-3), "ms_per_step": hier_ms,
-                     "refine_rate": refine, "speedup_vs_flat": flat_ms / hier_ms},
-            "false_dismissal": {"fp64_detections": n_det, "missed": missed_h,
-                                "rate": missed_h / n_det if n_det else 0.0,
-                                "injections": inj},
-            "roofline_flat": {"bound": "fp32", "achieved": flops / (flat_ms * 1e-3) / 1e12,
-                              "peak": peak.value / 1e12, "unit": "TFLOP/s",
-                              "frac": flops / (flat_ms * 1e-3) / peak.value,
-                              "flops_per_pair": FLOPS_PER_PAIR(LN),
-                              "peak_source": "measured FP32 FMA loop on this GPU"},
-            "cpu_baseline": cb,
-            "clocks": clocks,
-        }))
+        line = {"metric": LARGE_METRIC, "value": rec.pop("value"), "unit": "pairs/s",
+                "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": rec.pop("ms_per_step"), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded, generated on the device)",
+                "config": {"workload": rec.pop("workload"), "gate": rec.pop("gate")}}
+        line.update(rec)
+        print(json.dumps(line))
 
 
 def main():

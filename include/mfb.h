@@ -65,7 +65,10 @@ int mfb_set_stream(mfb_plan *p, void *stream);
 int mfb_set_data(mfb_plan *p, int d0, int count, const void *spec);
 int mfb_set_templates(mfb_plan *p, int t0, int count, const void *spec);
 /* Replaces ap_mf_run (src/matchfilt.c:411-420; matchedfilter.h:66-70).
-   idx: int64 [nd*nt*nb]; val: complex64 [nd*nt*nb]; counts: int32 [nd*nt] or NULL. */
+   idx: int64 [nd*nt*nb]; val: complex64 [nd*nt*nb]; counts: int32 [nd*nt] or NULL.
+   Returns 0, not the total of threshold crossings that ap_mf_run returns
+   (matchedfilter.h:66-71): the run is only enqueued here, and the total would
+   need a host synchronisation.  Sum `counts` after synchronising instead. */
 int mfb_run(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize, float threshold,
             size_t start, size_t end, int64_t *idx, void *val, int32_t *counts);
 /* Same as mfb_run, but the output is one array of 16-byte records laid out
@@ -82,7 +85,8 @@ int mfb_run_records(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
 int mfb_run_rows(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *rows,
                  const int32_t *nrows, int max_rows, size_t binsize, float threshold,
                  size_t start, size_t end, int64_t *idx, void *val, int32_t *counts);
-/* Replaces ap_mf_run_series (src/matchfilt.c:437-490; matchedfilter.h:98-103).
+/* Replaces ap_mf_run_series (src/matchfilt.c:437-490; matchedfilter.h:98-103);
+   returns 0, not the crossings total (see mfb_run).
    series: complex64 [nseries] (device or host); starts/win_start/win_end:
    host arrays of nblocks.  Every block's window must give the same bin count
    (MFB_ERR_ARG otherwise).  Block b's spectrum is FFT(series[start..start+n)/n),
@@ -124,7 +128,8 @@ int mfb_hier_set_reference(mfb_hplan *p, const float *power);
 int mfb_hier_set_threshold(mfb_hplan *p, float coarse_threshold);
 /* Replaces ap_hmf_run (src/hmf.c:222-328): coarse pass, gate, and a refine of
    the survivors with the flat kernel, all enqueued on the stream with no host
-   decision in between.  Same arguments and output as mfb_run. */
+   decision in between.  Same arguments and output as mfb_run; returns 0,
+   not the crossings total of ap_hmf_run (see mfb_run). */
 int mfb_hier_run(mfb_hplan *p, int d0, int nd, int t0, int nt, size_t binsize, float threshold,
                  size_t start, size_t end, int64_t *idx, void *val, int32_t *counts);
 /* mfb_hier_run with PEAK_DTYPE record output, as mfb_run_records. */
@@ -263,7 +268,14 @@ int mfb_adjoint(int device, size_t n, const void *data, int nd, const void *temp
 /* ---- large transforms with no allocation --------------------------------- */
 
 /* Size of the file-scope device array that mfb_run_large_static uses as its
-   scratch: 8 MiB per device, reserved when the library's device code loads. */
+   scratch: 8 MiB per device, reserved when the library's device code loads on
+   that device.  With CUDA's lazy module loading (the default) that load, and
+   so the reservation, happens at the first kernel launch of any mfb_* entry
+   point on the device -- which is the first mfb_run_large_static call itself
+   when nothing else has run there -- and the kernels a call launches may be
+   loaded (their code placed in device memory) at their own first launch.
+   Make one earlier call on the device, or set CUDA_MODULE_LOADING=EAGER, if
+   even that first reservation must happen before a given point. */
 #define MFB_STATIC_SCRATCH_BYTES (8u << 20)
 
 /* No counterpart in the reference.  The two-pass filter of mfb_run for

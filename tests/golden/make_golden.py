@@ -166,7 +166,9 @@ def make_gate(out, gate_for):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the reference tree>")
+    ref = sys.argv[1]
     spec = importlib.util.spec_from_file_location(
         "ref_gatemodel", os.path.join(ref, "python", "matchedfilter", "gatemodel.py"))
     gm = importlib.util.module_from_spec(spec)

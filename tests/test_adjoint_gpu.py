@@ -87,6 +87,10 @@ def test_value_gradient_and_forward_values():
     D = torch.from_numpy(Dn).cuda().requires_grad_(True)
     H = torch.from_numpy(Hn).cuda().requires_grad_(True)
     idx, val, power = peak_values(D, H, binsize)
+    from oracle import oracle, parity
+    bad = parity.compare(idx.cpu().numpy(), val.detach().cpu().numpy(),
+                         oracle.correlate(Dn, Hn), binsize)
+    assert not bad, bad[:3]
     f = mf.MatchedFilter(n, nd, nt)
     f.set_data(Dn)
     f.set_templates(Hn)

@@ -102,9 +102,14 @@ def test_pure_noise_is_ruled_out():
 
 @pytest.mark.parametrize("coarse", ["fp32", "bf16x3"])
 def test_omission_rate_meets_the_budget(coarse):
-    """False dismissal at the budget, 1500 trials in one batched run."""
+    """False dismissal within the budget fd, 16384 trials in one batched run
+    (signals at exactly snr in the gate model's own complex noise).  The
+    gate is the model's fd-quantile, so the measured rate is a binomial
+    estimate around a true rate of at most fd: the bound allows three
+    standard deviations of that estimate above fd (with ~8000 detections
+    that is fd + 0.3 fd), no more."""
     mf = _mf()
-    n, trials, snr, fd = 4096, 1500, 5.5, 1e-2
+    n, trials, snr, fd = 4096, 16384, 5.5, 1e-2
     rng = np.random.default_rng(13)
     power = inspiral_power(n)
     H = template_with_power(n, power)
@@ -122,8 +127,10 @@ def test_omission_rate_meets_the_budget(coarse):
     b = hf.run(binsize=n, threshold=snr)
     det = a["index"][:, 0, 0] >= 0
     omitted = det & (b["index"][:, 0, 0] < 0)
-    rate = omitted.sum() / max(det.sum(), 1)
-    assert rate <= 3 * fd, (rate, det.sum())
+    ndet = int(det.sum())
+    assert ndet > 4000
+    bound = fd * ndet + 3.0 * np.sqrt(fd * (1 - fd) * ndet)
+    assert omitted.sum() <= bound, (int(omitted.sum()), ndet, bound)
 
 
 def test_calibration_contract():

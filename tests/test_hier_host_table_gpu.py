@@ -241,3 +241,129 @@ def test_host_table_other_kinds_and_lengths(n, band, coarse):
         assert hit.any()
         assert not parity.compare(out["index"], out["value"], oracle.correlate(D, H), bs, 0.0,
                                   (n // 32, n - 7), rows_mask=hit)
+
+
+def _injected(rng, n, nd, H, pairs, amp=50.0):
+    """Complex unit-variance noise plus `amp` * H[t] at a random lag on data
+    row d for every (d, t) in pairs: with a coarse gate of 10 only those
+    pairs fire (their coarse maximum is about amp * sqrt(band/n))."""
+    D = (rng.standard_normal((nd, n)) + 1j * rng.standard_normal((nd, n))) / np.sqrt(2)
+    k = np.arange(n)
+    for d, t in pairs:
+        lag = int(rng.integers(n))
+        D[d] += amp * H[t].astype(np.complex128) * np.exp(-2j * np.pi * k * lag / n)
+    return D.astype(np.complex64)
+
+
+def test_row_marks_over_survivor_sets():
+    """Survivor sets A, A|B, B, A, then A, A|B, B again through the replayed
+    graph (same pinned bank, new contents): every table equals the dense run,
+    and the bytes written are (rows reset + rows refined) * nb * 16 -- a row
+    refined in consecutive runs is written each time it is refined and never
+    reset in between; a row refined, dropped and refined again is reset once
+    and written again."""
+    import torch
+    n, nd, nt, band, bs = 4096, 4, 32, 512, 512
+    nb = n // bs
+    rng = np.random.default_rng(31)
+    H = noise(rng, (nt, n))
+    H /= np.linalg.norm(H, axis=1, keepdims=True)
+    hf = _filter(n, nd, nt, band, "bf16x3", 10.0)
+    hf.set_templates(H)
+    A = {(0, 1), (1, 5), (2, 7)}
+    B = {(0, 3), (3, 9), (2, 20)}
+    pin = torch.empty((nd, n), dtype=torch.complex64, pin_memory=True)
+    sequence = [A, A | B, B, A, A, A | B, B]
+    prev = None
+    for k, S in enumerate(sequence):
+        D = _injected(rng, n, nd, H, sorted(S))
+        if k >= 4:                                 # same pinned bank: graph capture and replay
+            pin.numpy()[:] = D
+            hf.set_data(pin.numpy())
+        else:
+            hf.set_data(D.copy())
+        out = hf.run(binsize=bs, threshold=5.0)
+        assert hf.last_refinements == len(S)
+        fired = {(int(d), int(t)) for d, t in zip(*np.nonzero((out["index"] >= 0).any(-1)))}
+        assert fired == S, (k, fired, S)
+        idx, val = _dense(hf, binsize=bs, threshold=5.0)
+        np.testing.assert_array_equal(out["index"], idx)
+        np.testing.assert_array_equal(out["value"], val)
+        if prev is None:
+            assert hf.last_d2h_bytes == nd * nt * nb * 16     # first table: copied whole
+        else:
+            assert hf.last_d2h_bytes == (len(prev - S) + len(S)) * nb * 16, (k, hf.last_d2h_bytes)
+        prev = S
+
+
+def test_replayed_run_follows_template_and_reference_changes():
+    """After identical calls have captured the run as a graph, changing the
+    template bank, the reference profile or the gate between two calls with
+    the same arguments must give the new answer."""
+    import torch
+    import apogee_b200 as mf
+    n, nd, nt, band, bs = 4096, 3, 24, 512, 256
+    rng = np.random.default_rng(32)
+    H1, H2 = noise(rng, (nt, n)), noise(rng, (nt, n))
+    hf = _filter(n, nd, nt, band, "bf16x3", 0.0)
+    hf.set_templates(H1)
+    pin = torch.empty((nd, n), dtype=torch.complex64, pin_memory=True)
+    D = noise(rng, (nd, n))
+    pin.numpy()[:] = D
+    for _ in range(3):                            # direct, capture, replay
+        hf.set_data(pin.numpy())
+        out = hf.run(binsize=bs)
+    assert not parity.compare(out["index"], out["value"], oracle.correlate(D, H1), bs)
+    hf.set_templates(H2)
+    for _ in range(3):
+        hf.set_data(pin.numpy())
+        out = hf.run(binsize=bs)
+        assert not parity.compare(out["index"], out["value"], oracle.correlate(D, H2), bs)
+    # a gate that dismisses some pairs, then a reference profile that rescales
+    # the coarse templates: the fired set must follow both
+    cv = hf.coarse_values()
+    g = float(np.quantile(cv, 0.5))
+    hf.set_coarse_threshold(g)
+    for _ in range(3):
+        hf.set_data(pin.numpy())
+        out = hf.run(binsize=bs)
+    fired = (out["index"] >= 0).any(-1)
+    np.testing.assert_array_equal(fired, (cv >= g))
+    power = np.ones(n, np.float32)
+    power[:band] = 4.0                            # in-band fraction 4/11 instead of each row's own
+    hf.set_reference(power)
+    cv2 = hf.coarse_values()
+    assert not np.allclose(cv2, cv)
+    for _ in range(2):
+        hf.set_data(pin.numpy())
+        out = hf.run(binsize=bs)
+        fired = (out["index"] >= 0).any(-1)
+        np.testing.assert_array_equal(fired, (cv2 >= g))
+    flat = mf.MatchedFilter(n, nd, nt)
+    flat.set_data(D)
+    flat.set_templates(H2)
+    ref = flat.run(binsize=bs)
+    np.testing.assert_array_equal(out[fired], ref[fired])
+
+
+def test_kept_results_follow_the_reuse_contract():
+    """run() reuses its result table, as the reference's run does
+    (python/matchedfilter/__init__.py:463-466, "The next run on this filter
+    overwrites it in place; .copy() anything that must outlive that call"):
+    a kept result shows the latest run, a copy keeps its own."""
+    n, nd, nt, bs = 4096, 2, 8, 1024
+    rng = np.random.default_rng(33)
+    H = noise(rng, (nt, n))
+    hf = _filter(n, nd, nt, 512, "bf16x3", 0.0)
+    hf.set_templates(H)
+    D1, D2 = noise(rng, (nd, n)), noise(rng, (nd, n))
+    hf.set_data(D1)
+    first = hf.run(binsize=bs)
+    first_copy = first.copy()
+    hf.set_data(D2)
+    second = hf.run(binsize=bs)
+    assert not parity.compare(second["index"], second["value"], oracle.correlate(D2, H), bs)
+    assert not parity.compare(first_copy["index"], first_copy["value"],
+                              oracle.correlate(D1, H), bs)
+    np.testing.assert_array_equal(first, second)          # the reused table
+    assert not (first_copy["index"] == second["index"]).all()

@@ -48,6 +48,11 @@ class OracleEngine:
         self.trig += int((idx >= 0).any(-1).sum())
         return out
 
+    def run_records(self, binsize=None, threshold=0.0, window=None):
+        import torch
+        out = self.run(binsize, threshold, window)
+        return torch.from_numpy(out.view(np.int64).reshape(out.shape + (2,)).copy())
+
     @property
     def stats(self):
         return self.pairs, self.trig
@@ -74,6 +79,9 @@ def _rank_main(rank, world, port, case, out_dir):
         f.set_data(D)
         f.set_templates(H)
         full = f.run(binsize=bs, threshold=thr)
+        rec = f.run_records(binsize=bs, threshold=thr)
+        assert tuple(rec.shape) == full.shape + (2,)
+        np.testing.assert_array_equal(rec.numpy().view(PEAK_DTYPE)[..., 0], full)
         pairs, trig = f.stats
         np.save(os.path.join(out_dir, "r%d.npy" % rank), full)
         np.save(os.path.join(out_dir, "s%d.npy" % rank), np.array([pairs, trig]))
@@ -99,5 +107,5 @@ def test_two_gloo_ranks_assemble_the_full_table(tmp_path, case):
         np.testing.assert_array_equal(full["index"], idx)
         np.testing.assert_array_equal(full["value"], val.astype(np.complex64))
         pairs, trig = np.load(tmp_path / ("s%d.npy" % r))
-        assert pairs == nd * nt
-        assert trig == int((idx >= 0).any(-1).sum())
+        assert pairs == 2 * nd * nt                 # run and run_records
+        assert trig == 2 * int((idx >= 0).any(-1).sum())

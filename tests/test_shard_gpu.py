@@ -46,8 +46,15 @@ def _rank_main(rank, port, out_dir):
         h.set_data(D)
         h.set_templates(H)
         c = h.run(binsize=256)
+        # the device-resident assembly: records stay on the GPU
+        rec = f.run_records(binsize=256)
+        hrec = h.run_records(binsize=256)
+        dev_ok = rec.is_cuda and hrec.is_cuda
+        r = rec.cpu().numpy().view(mf.PEAK_DTYPE)[..., 0]
+        hr = hrec.cpu().numpy().view(mf.PEAK_DTYPE)[..., 0]
         np.save(os.path.join(out_dir, "ok.npy"), np.array([
-            int(np.array_equal(a, b)), int(np.array_equal(c, b)), *h.stats]))
+            int(np.array_equal(a, b)), int(np.array_equal(c, b)),
+            int(dev_ok and np.array_equal(r, b) and np.array_equal(hr, b)), *h.stats]))
     finally:
         dist.destroy_process_group()
 
@@ -56,6 +63,6 @@ def test_one_nccl_rank_matches_plain_filter(tmp_path):
     import torch.multiprocessing as mp
     mp.start_processes(_rank_main, args=(_free_port(), str(tmp_path)), nprocs=1, join=True,
                        start_method="spawn")
-    flat_ok, hier_ok, pairs, trig = np.load(tmp_path / "ok.npy")
-    assert flat_ok == 1 and hier_ok == 1
-    assert pairs == 27 and trig == 27
+    flat_ok, hier_ok, rec_ok, pairs, trig = np.load(tmp_path / "ok.npy")
+    assert flat_ok == 1 and hier_ok == 1 and rec_ok == 1
+    assert pairs == 54 and trig == 54
