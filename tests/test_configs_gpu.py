@@ -227,8 +227,9 @@ def test_large_bank_subsample_config4():
         bad += parity.compare(out["index"][:, t0:t0 + 8], out["value"][:, t0:t0 + 8], z,
                               binsize, thr)
     assert not bad, bad[:5]
+    lobe = n // 2048                 # the main lobe widens with n (64 lags here)
     for d, t, lag, snr in inj:
-        assert abs(int(out["index"][d, sel.index(t), lag // binsize]) - lag) <= 8
+        assert abs(int(out["index"][d, sel.index(t), lag // binsize]) - lag) <= lobe
     hf = mf.HierarchicalFilter(n, 4, len(sel), snr=6.0, fd=1e-3, band=n // 16, coarse="fp32")
     hf.set_reference(pn)
     hf.set_templates(H)
@@ -237,7 +238,7 @@ def test_large_bank_subsample_config4():
     rows = (hout["index"] >= 0).any(-1)
     np.testing.assert_array_equal(hout[rows], out[rows])
     for d, t, lag, snr in inj:
-        assert abs(int(hout["index"][d, sel.index(t), lag // binsize]) - lag) <= 8
+        assert abs(int(hout["index"][d, sel.index(t), lag // binsize]) - lag) <= lobe
     del f, hf
     torch.cuda.empty_cache()
 
