@@ -20,6 +20,7 @@
 #include <cstddef>
 #include "../../include/mfb.h"
 #include "flat_kernel.cuh"
+#include "flat2_kernel.cuh"
 #include "series_kernel.cuh"
 #include "hier_kernels.cuh"
 #include "large_kernel.cuh"
@@ -99,6 +100,9 @@ struct NConst {
   int grid_peaks = 0, grid_gate = 0, grid_fwd = 0;
   int cta = 0, smem = 0, g = 0;
   int grid_rows = 0;
+  // n = 4096: the two-pairs-per-thread kernel (flat2_kernel.cuh)
+  float4 *twid2 = nullptr;      // Flat2Geo::TW records (wr, wr, wi, wi)
+  int grid2 = 0;
 };
 static std::mutex g_const_mu;
 static std::map<std::pair<int, int>, NConst> g_const;
@@ -132,6 +136,20 @@ static int make_const(int device, NConst &c) {
                                                          Geo::SMEM));
   if (b1 < 1 || b2 < 1 || b3 < 1 || b4 < 1)
     return fail(MFB_ERR_CUDA, "kernel for n=%d cannot be resident on this device", N);
+  if constexpr (N == Flat2Geo::N) {
+    // the scalar tables' values, duplicated for the two lanes
+    std::vector<float4> tw2(Flat2Geo::TW);
+    for (int i = 0; i < Flat2Geo::TW; i++) tw2[i] = make_float4(tw[i].x, tw[i].x, tw[i].y, tw[i].y);
+    CUDA_TRY(cudaMalloc(&c.twid2, tw2.size() * sizeof(float4)));
+    CUDA_TRY(cudaMemcpy(c.twid2, tw2.data(), tw2.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaFuncSetAttribute(flat2_kernel<MODE_PEAKS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, Flat2Geo::SMEM));
+    int b5 = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b5, flat2_kernel<MODE_PEAKS>,
+                                                           Flat2Geo::T, Flat2Geo::SMEM));
+    if (b5 < 1) return fail(MFB_ERR_CUDA, "packed kernel for n=%d cannot be resident", N);
+    c.grid2 = b5 * sms;
+  }
   c.grid_rows = b4 * sms;
   c.grid_peaks = b1 * sms;
   c.grid_gate = b2 * sms;
@@ -173,6 +191,20 @@ static cudaError_t launch_flat(int n, const NConst &c, const FlatArgs &a, cudaSt
 #undef MFB_CASE
     default: return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+// The two-pairs-per-thread kernel covers n = 4096 peaks over the whole lag
+// window with bins a multiple of 32 lags and at most KEYCAP bins, dense or
+// listed; it gives the same bits as flat_kernel / rows_kernel.
+static bool flat2_applies(int n, const NConst &c, const FlatArgs &a) {
+  return n == Flat2Geo::N && c.twid2 && a.ws == 0 && a.we == n && (a.binsize & 31) == 0 &&
+         a.nb <= KEYCAP;
+}
+
+static cudaError_t launch_flat2(const NConst &c, FlatArgs a, cudaStream_t s) {
+  a.twid = reinterpret_cast<const float2 *>(c.twid2);
+  flat2_kernel<MODE_PEAKS><<<c.grid2, Flat2Geo::T, Flat2Geo::SMEM, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -357,6 +389,7 @@ struct mfb_plan {
   float2 *lY = nullptr;
   uint4 *lrec = nullptr;
   int lbatch = 0;
+  int packed = 1;           // use flat2_kernel where it applies (mfb_set_packed)
 };
 
 struct DeviceGuard {
@@ -550,7 +583,16 @@ static int run_impl(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
   if (is_large(p->n))
     return run_large(p, d0, nd, t0, nt, nullptr, 0, binsize, threshold, start, end, nb, idx, val,
                      counts, rs);
-  CUDA_TRY(launch_flat<MODE_PEAKS>((int)p->n, *p->c, a, p->stream));
+  if (p->packed && flat2_applies((int)p->n, *p->c, a))
+    CUDA_TRY(launch_flat2(*p->c, a, p->stream));
+  else
+    CUDA_TRY(launch_flat<MODE_PEAKS>((int)p->n, *p->c, a, p->stream));
+  return MFB_OK;
+}
+
+extern "C" int mfb_set_packed(mfb_plan *p, int on) {
+  if (!p) return fail(MFB_ERR_ARG, "null plan");
+  p->packed = on ? 1 : 0;
   return MFB_OK;
 }
 
@@ -595,7 +637,10 @@ static int run_rows_impl(mfb_plan *p, int d0, int nd, int t0, int nt, const int3
     return run_large(p, d0, nd, t0, nt, rows, cnt, binsize, threshold, start, end, nb, idx, val,
                      counts, rs);
   }
-  CUDA_TRY(launch_rows((int)p->n, *p->c, a, p->stream));
+  if (p->packed && flat2_applies((int)p->n, *p->c, a))
+    CUDA_TRY(launch_flat2(*p->c, a, p->stream));
+  else
+    CUDA_TRY(launch_rows((int)p->n, *p->c, a, p->stream));
   return MFB_OK;
 }
 
@@ -858,6 +903,12 @@ static void hier_drop_graph(mfb_hplan *h) {
     cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
   }
+}
+
+extern "C" int mfb_hier_set_packed(mfb_hplan *h, int on) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  hier_drop_graph(h);
+  return mfb_set_packed(h->full, on);
 }
 
 extern "C" int mfb_hier_set_stream(mfb_hplan *h, void *stream) {

@@ -78,6 +78,14 @@ int mfb_run(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize, float t
    device). records: DEVICE [nd*nt*nb] x 16 bytes. */
 int mfb_run_records(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize, float threshold,
                     size_t start, size_t end, void *records, int32_t *counts);
+/* Kernel choice for n = 4096 (no counterpart in the reference, whose CPU
+   engine picks its own code path per shape): on (the default), runs whose
+   lag window is [0, n) with bins a multiple of 32 lags and at most 64 bins
+   use the kernel that carries two pairs per thread in packed FP32x2
+   arithmetic; off, they use the one-pair-per-thread kernel.  Both compute
+   the same operations in the same order and give bit-identical results;
+   the switch lets a caller compare or time the two. */
+int mfb_set_packed(mfb_plan *p, int on);
 /* Replaces ap_mf_run_sel (src/matchfilt.c:492-503) in list form: run only the
    output rows rows[0..*nrows) of the block [d0,d0+nd) x [t0,t0+nt), where a row
    is (d-d0)*nt + (t-t0) and the row count lives in DEVICE memory (nrows), so a
@@ -115,6 +123,8 @@ int mfb_supported(size_t n);
 int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, size_t band,
                     int coarse_kind, int device);
 int mfb_hier_destroy(mfb_hplan *p);
+/* mfb_set_packed for the plan's refine (and its flat filter). */
+int mfb_hier_set_packed(mfb_hplan *p, int on);
 int mfb_hier_set_stream(mfb_hplan *p, void *stream);
 /* Replaces ap_hmf_set_data / ap_hmf_set_template (src/hmf.c:139-156).  The
    template's band fraction is summed in FP64 on the device. */

@@ -282,3 +282,74 @@ def test_batch_independence():
     g.set_templates(H[5:6])
     one = g.run(binsize=512)
     np.testing.assert_array_equal(one[0, 0], full[3, 5])
+
+
+def _same_up_to_near_ties(i1, i2, z):
+    """Indices equal except where the two lags' FP64 magnitudes are within
+    1e-5 relative (either kernel may then report either lag)."""
+    diff = np.nonzero(i1 != i2)
+    for pos in zip(*diff):
+        a, b = i1[pos], i2[pos]
+        assert a >= 0 and b >= 0, pos
+        za, zb = abs(z[pos[:-1]][a]), abs(z[pos[:-1]][b])
+        assert abs(za - zb) <= 1e-5 * max(za, zb), (pos, a, b, za, zb)
+
+
+@pytest.mark.parametrize("nd,nt,binsize,threshold", [
+    (16, 1024, 256, 0.0),     # the benchmark block: data rows shared by both pairs of an item
+    (5, 77, 512, 3.0),        # odd nt: items straddle data rows; thresholded
+    (3, 1, 64, 0.0),          # one template: every item mixes data rows; 64 bins
+    (1, 3, 4096, 2.0),        # odd pair count: the last item's second pair is absent
+])
+def test_packed_kernel_matches_one_pair_kernel_and_oracle(nd, nt, binsize, threshold):
+    """n = 4096 runs over the whole window use the kernel that carries two
+    pairs per thread in packed FP32x2 arithmetic.  It must meet the oracle's
+    bar and agree with the one-pair kernel (dense, listed and record output,
+    counts), indices up to FP64 near-ties; listed rows equal the dense run's
+    rows bit for bit."""
+    import torch
+    import apogee_b200 as mf
+    from apogee_b200 import _lib
+    n = 4096
+    rng = np.random.default_rng(nd * 100 + nt)
+    D = noise(rng, (nd, n))
+    H = noise(rng, (nt, n))
+    f = mf.MatchedFilter(n, nd, nt)
+    f.set_data(D)
+    f.set_templates(H)
+    L = _lib.lib()
+    out = {}
+    for packed in (0, 1):
+        _lib.check(L.mfb_set_packed(f._plan, packed))
+        r, c = f.run(binsize=binsize, threshold=threshold, counts=True)
+        ri, rv = f.run(binsize=binsize, threshold=threshold, raw=True)
+        out[packed] = (r.copy(), c.copy(), ri.copy(), rv.copy())
+        np.testing.assert_array_equal(out[packed][0]["index"], out[packed][2])
+        np.testing.assert_array_equal(out[packed][0]["value"], out[packed][3])
+        np.testing.assert_array_equal(out[packed][1], (out[packed][2] >= 0).sum(-1))
+    for t0 in range(0, nt, 128):
+        z = oracle.correlate(D, H[t0:t0 + 128])
+        for packed in (0, 1):
+            r = out[packed][0][:, t0:t0 + 128]
+            bad = parity.compare(r["index"], r["value"], z, binsize, threshold)
+            assert not bad, (packed, bad[:3])
+        _same_up_to_near_ties(out[0][2][:, t0:t0 + 128], out[1][2][:, t0:t0 + 128], z)
+    # listed rows in arbitrary order, an odd count
+    rows = np.random.default_rng(7).permutation(nd * nt)[: max(1, (nd * nt) // 2) | 1]
+    rows_d = torch.as_tensor(rows.astype(np.int32), device="cuda")
+    cnt_d = torch.tensor([rows.size], dtype=torch.int32, device="cuda")
+    nb = n // binsize
+    _lib.check(L.mfb_set_packed(f._plan, 1))
+    f._bind_stream()
+    idx = torch.full((nd * nt * nb,), -7, dtype=torch.int64, device="cuda")
+    val = torch.zeros(nd * nt * nb, dtype=torch.complex64, device="cuda")
+    _lib.check(L.mfb_run_rows(f._plan, 0, nd, 0, nt, rows_d.data_ptr(), cnt_d.data_ptr(),
+                              rows.size, binsize, threshold, 0, n, idx.data_ptr(),
+                              val.data_ptr(), None))
+    torch.cuda.synchronize()
+    got_i = idx.cpu().numpy().reshape(nd * nt, nb)
+    got_v = val.cpu().numpy().reshape(nd * nt, nb)
+    np.testing.assert_array_equal(got_i[rows], out[1][2].reshape(nd * nt, nb)[rows])
+    np.testing.assert_array_equal(got_v[rows], out[1][3].reshape(nd * nt, nb)[rows])
+    untouched = np.setdiff1d(np.arange(nd * nt), rows)
+    assert (got_i[untouched] == -7).all()
