@@ -477,18 +477,21 @@ class MatchedFilter:
         self.clear_cache()
 
 
-#: Bands the split-precision tensor-core coarse pass covers.
-TC_BANDS = frozenset([512])
+#: Bands the split-precision tensor-core coarse pass covers: 512 directly,
+#: 16384 as a four-step around the 512-point pass.
+TC_BANDS = frozenset([512, 16384])
+#: Bands at which coarse="auto" takes the tensor-core pass.
+AUTO_TC_BANDS = frozenset([512])
 
 
 def _coarse_kind(name, band=None):
     """Library coarse kind for `name` at `band` ("auto": the BF16 split
-    tensor-core pass where it covers the band, else the FP32 pass)."""
+    tensor-core pass at AUTO_TC_BANDS, else the FP32 pass)."""
     kinds = {"bf16x3": _lib.COARSE_BF16X3, "fp16x3": _lib.COARSE_FP16X3, "fp32": _lib.COARSE_FP32}
     if name == "auto":
         if band is None:
             return None
-        return _lib.COARSE_BF16X3 if band in TC_BANDS else _lib.COARSE_FP32
+        return _lib.COARSE_BF16X3 if band in AUTO_TC_BANDS else _lib.COARSE_FP32
     if name not in kinds:
         raise ValueError("coarse must be one of %s" % sorted(list(kinds) + ["auto"]))
     return kinds[name]
@@ -507,8 +510,8 @@ class HierarchicalFilter(MatchedFilter):
     ``coarse`` picks the coarse arithmetic: ``"bf16x3"`` / ``"fp16x3"``
     (split hi+lo tensor-core contraction, FP32 accumulation), ``"fp32"``
     (the flat FP32 kernel at length band, the reference's own method), or
-    ``"auto"`` (default): the BF16 split tensor-core pass at the bands it
-    covers (TC_BANDS), the FP32 pass at the others.
+    ``"auto"`` (default): the BF16 split tensor-core pass at AUTO_TC_BANDS,
+    the FP32 pass at the others.  The tensor-core kinds cover TC_BANDS.
     """
 
     def __init__(self, n, ndata=1, ntemplates=1, snr=5.5, fd=1e-2,

@@ -36,6 +36,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cmath>
+#include <climits>
 #include <cstring>
 #include <vector>
 #include "hier_kernels.cuh"
@@ -153,6 +154,12 @@ struct TcKernelArgs {
   int32_t *fire_list, *fire_count;
   float *coarse_out;
   int *err;
+  // Rows mode (the band-16384 four-step): "pairs" are rows r of a scratch of
+  // already-formed 512-point products (data = the scratch, nd = rows, nt = 1,
+  // no template), row r is column k2 = r % rows_n2 of a longer band whose
+  // lags are rows_n2 * j + k2; the window [cs, ce) is on that longer grid,
+  // and coarse_out receives max |z|^2 of the row (no gate).
+  int rows_n2, cs, ce;
 };
 
 // Warp-specialised form of the same pass: three roles in one 512-thread CTA
@@ -255,7 +262,12 @@ coarse_tc_ws_kernel(const TcKernelArgs a) {
     float2 pd[16], ph[16];
     auto issue_loads = [&](int it) {
       const long long pi = (ibeg + it) * PAIRS + warp;
-      if (it < nit && pi < total) {
+      if (it < nit && pi < total && a.rows_n2 > 0) {
+        // rows mode: the product is already formed (times conj(1) below, exact)
+        const float2 *dp = a.data + pi * (long long)a.data_stride;
+#pragma unroll
+        for (int f1 = 0; f1 < 16; f1++) { pd[f1] = __ldg(dp + 32 * f1 + lane); ph[f1] = make_float2(1.f, 0.f); }
+      } else if (it < nit && pi < total) {
         const int d = (int)(pi / a.nt), t = (int)(pi - (long long)d * a.nt);
         const float2 *dp = a.data + (long long)(a.d0 + d) * a.data_stride;
         const float2 *hp = a.ct + (long long)(a.t0 + t) * BAND;
@@ -393,6 +405,14 @@ coarse_tc_ws_kernel(const TcKernelArgs a) {
       const uint32_t u = (uint32_t)(it / NSLOT);
       mbar_wait_ab(bar(tcw::B_FULL2 + k), u & 1, abort_flag, a.err);                       // S2[k] full
       tc_after_sync();
+      int ws = a.ws, we = a.we;
+      if (a.rows_n2 > 0) {
+        // lags rows_n2 * j + k2 of the longer band inside [cs, ce)
+        const long long pi = (ibeg + it) * PAIRS + (R >> 4);
+        const int k2 = (int)(pi % a.rows_n2);
+        ws = a.cs > k2 ? (a.cs - k2 + a.rows_n2 - 1) / a.rows_n2 : 0;
+        we = a.ce > k2 ? (a.ce - k2 + a.rows_n2 - 1) / a.rows_n2 : 0;
+      }
       float best = 0.f;
 #pragma unroll
       for (int half = 0; half < 2; half++) {
@@ -404,7 +424,7 @@ coarse_tc_ws_kernel(const TcKernelArgs a) {
           const float zr = __uint_as_float(v[2 * jj]), zi = __uint_as_float(v[2 * jj + 1]);
           const int j = j1 + 16 * (16 * half + jj);
           const float m2 = fmaf(zr, zr, zi * zi);
-          if (j >= a.ws && j < a.we && m2 > best) best = m2;
+          if (j >= ws && j < we && m2 > best) best = m2;
         }
       }
       tc_before_sync();
@@ -415,7 +435,9 @@ coarse_tc_ws_kernel(const TcKernelArgs a) {
       const long long pi = (ibeg + it) * PAIRS + pr;
       if (pi < total && !*abort_flag) {
         const int row = (int)pi;
-        if (a.coarse_out) {
+        if (a.rows_n2 > 0) {
+          if ((lane & 15) == 0) a.coarse_out[pi] = best;
+        } else if (a.coarse_out) {
           if ((lane & 15) == 0) a.coarse_out[row] = sqrtf(best);
         } else {
           const bool fire = best > a.t2 && sqrtf(best) >= a.gate;
@@ -574,6 +596,26 @@ int tc_coarse_run(TcCoarse *c, const TcRunArgs &r, cudaStream_t s) {
   a.fire_count = r.fire_count;
   a.coarse_out = r.coarse_out;
   a.err = c->err;
+  if (c->fp16) coarse_tc_ws_kernel<1><<<c->grid, tcw::THREADS, tcw::SMEM_BYTES, s>>>(a);
+  else coarse_tc_ws_kernel<0><<<c->grid, tcw::THREADS, tcw::SMEM_BYTES, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { g_tc_err = cudaGetErrorString(e); return -1; }
+  return 0;
+}
+
+int tc_coarse_rows(TcCoarse *c, const float2 *rows, long long nrows, int n2, int cs, int ce,
+                   float *m2_out, cudaStream_t s) {
+  if (!c) { g_tc_err = "no tensor-core coarse state"; return -1; }
+  if (nrows < 1 || nrows > INT_MAX || n2 < 1) { g_tc_err = "invalid row count"; return -1; }
+  TcKernelArgs a;
+  memset(&a, 0, sizeof a);
+  a.data = rows;
+  a.data_stride = tc::BAND;
+  a.consts = c->consts;
+  a.d0 = 0; a.nd = (int)nrows; a.t0 = 0; a.nt = 1;
+  a.coarse_out = m2_out;
+  a.err = c->err;
+  a.rows_n2 = n2; a.cs = cs; a.ce = ce;
   if (c->fp16) coarse_tc_ws_kernel<1><<<c->grid, tcw::THREADS, tcw::SMEM_BYTES, s>>>(a);
   else coarse_tc_ws_kernel<0><<<c->grid, tcw::THREADS, tcw::SMEM_BYTES, s>>>(a);
   cudaError_t e = cudaGetLastError();

@@ -233,6 +233,11 @@ int tc_coarse_create(TcCoarse **out, int m, int ntmpl, int ndata, int fp16);
 void tc_coarse_destroy(TcCoarse *c);
 int tc_coarse_pack_templates(TcCoarse *c, const float2 *ct, int t0, int count, cudaStream_t s);
 int tc_coarse_run(TcCoarse *c, const TcRunArgs &a, cudaStream_t s);
+// Rows mode of the same pass: max |z|^2 of the 512-point inverse DFT of each
+// of `nrows` already-formed rows (stride 512), row r being column r % n2 of a
+// band of 512 * n2 points whose lags n2 * j + (r % n2) are kept in [cs, ce).
+int tc_coarse_rows(TcCoarse *c, const float2 *rows, long long nrows, int n2, int cs, int ce,
+                   float *m2_out, cudaStream_t s);
 const char *tc_coarse_error();
 // 0, or -1 if a run timed out waiting for the tensor cores (synchronous).
 int tc_coarse_check(TcCoarse *c);

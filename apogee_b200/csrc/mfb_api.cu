@@ -23,6 +23,7 @@
 #include "flat2_kernel.cuh"
 #include "series_kernel.cuh"
 #include "hier_kernels.cuh"
+#include "band_kernels.cuh"
 #include "large_kernel.cuh"
 #include "adjoint_kernel.cuh"
 #include "batch_kernel.cuh"
@@ -809,6 +810,12 @@ struct mfb_hplan {
   bool last_valid = false;
   cudaGraphExec_t graph = nullptr;
   cudaStream_t cap = nullptr;
+  // band 16384 on the tensor cores (band_kernels.cuh): a batch of pairs'
+  // 32 x 512 scratch, their row maxima, and the four-step's twiddles
+  float2 *bY = nullptr;
+  float *bM2 = nullptr;
+  float2 *bw32 = nullptr, *bwm = nullptr;
+  int bbatch = 0;
 };
 
 extern "C" int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, size_t band,
@@ -854,8 +861,33 @@ extern "C" int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, 
     if (e == cudaSuccess) e = cudaMemset(h->fpow, 0, (size_t)ntmpl * sizeof(float));
   }
   if (r == MFB_OK && e == cudaSuccess && coarse_kind != MFB_COARSE_FP32) {
-    r = tc_coarse_create(&h->tc, (int)band, ntmpl, ndata, coarse_kind == MFB_COARSE_FP16X3);
-    if (r != 0) { r = fail(MFB_ERR_CUDA, "tensor-core coarse setup failed: %s", tc_coarse_error()); }
+    if (band != (size_t)BAND_COLS && band != (size_t)BAND_BIG) {
+      r = fail(MFB_ERR_UNSUPPORTED, "the tensor-core coarse pass covers band 512 and 16384, not %zu",
+               band);
+    } else {
+      r = tc_coarse_create(&h->tc, BAND_COLS, ntmpl, ndata, coarse_kind == MFB_COARSE_FP16X3);
+      if (r != 0) r = fail(MFB_ERR_CUDA, "tensor-core coarse setup failed: %s", tc_coarse_error());
+    }
+    if (r == MFB_OK && band == (size_t)BAND_BIG) {
+      // 512 pairs per batch: a 64 MiB scratch that stays in L2 between the passes
+      h->bbatch = (int)std::min<long long>(512, (long long)ndata * ntmpl);
+      e = cudaMalloc(&h->bY, (size_t)h->bbatch * BAND_BIG * sizeof(float2));
+      if (e == cudaSuccess) e = cudaMalloc(&h->bM2, (size_t)h->bbatch * BAND_ROWS * sizeof(float));
+      if (e == cudaSuccess) e = cudaMalloc(&h->bw32, 16 * sizeof(float2));
+      if (e == cudaSuccess) e = cudaMalloc(&h->bwm, 256 * sizeof(float2));
+      if (e == cudaSuccess) {
+        // W_16384^m = W^(128 (m >> 7)) * W^(m & 127): low table, then high table
+        std::vector<float2> w32(16), wm(256);
+        for (int k = 0; k < 16; k++) w32[k] = unit_root(k, BAND_ROWS);
+        for (int i = 0; i < 128; i++) {
+          wm[i] = unit_root(i, BAND_BIG);
+          wm[128 + i] = unit_root(128LL * i, BAND_BIG);
+        }
+        e = cudaMemcpy(h->bw32, w32.data(), 16 * sizeof(float2), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+          e = cudaMemcpy(h->bwm, wm.data(), 256 * sizeof(float2), cudaMemcpyHostToDevice);
+      }
+    }
   }
   if (r != MFB_OK || e != cudaSuccess) {
     if (r == MFB_OK) r = fail(MFB_ERR_CUDA, "hierarchical plan allocation failed: %s",
@@ -888,6 +920,10 @@ extern "C" int mfb_hier_destroy(mfb_hplan *h) {
   if (h->cap) cudaStreamDestroy(h->cap);
   free(h->tready);
   tc_coarse_destroy(h->tc);
+  cudaFree(h->bY);
+  cudaFree(h->bM2);
+  cudaFree(h->bw32);
+  cudaFree(h->bwm);
   delete h;
   return MFB_OK;
 }
@@ -1017,6 +1053,55 @@ __global__ void accumulate_triggers(const int32_t *count, unsigned long long *to
   *total += (unsigned long long)*count;
 }
 
+// The band-16384 tensor-core coarse pass over the block (band_kernels.cuh):
+// per batch of pairs, the column pass, the 512-point tensor-core pass over the
+// scratch rows, and the per-pair maximum with the gate (or, with coarse_out,
+// the coarse values).
+static int band_big_coarse(mfb_hplan *h, int d0, int nd, int t0, int nt, int cs, int ce,
+                           int64_t *idx, void *val, int rs, size_t full_nb, float *coarse_out,
+                           cudaStream_t s) {
+  mfb_plan *p = h->full;
+  const long long total = (long long)nd * nt;
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+  for (long long p0 = 0; p0 < total; p0 += h->bbatch) {
+    const int batch = (int)std::min<long long>(h->bbatch, total - p0);
+    BandColArgs c;
+    c.data = p->data;
+    c.data_stride = (long long)h->n;
+    c.ct = h->ct;
+    c.d0 = d0; c.nd = nd; c.t0 = t0; c.nt = nt;
+    c.pair0 = p0;
+    c.batch = batch;
+    c.w32 = h->bw32;
+    c.wm = h->bwm;
+    c.Y = h->bY;
+    const int gc = (int)std::min<long long>(2LL * batch, 8LL * sms);
+    band_col_kernel<<<gc, 256, 0, s>>>(c);
+    CUDA_TRY(cudaGetLastError());
+    if (tc_coarse_rows(h->tc, h->bY, (long long)batch * BAND_ROWS, BAND_ROWS, cs, ce, h->bM2, s))
+      return fail(MFB_ERR_CUDA, "tensor-core coarse pass failed: %s", tc_coarse_error());
+    BandGateArgs g;
+    g.m2 = h->bM2;
+    g.pair0 = p0;
+    g.batch = batch;
+    g.nt = nt;
+    g.total = total;
+    g.t2 = h->cal_thr > 0.f ? h->cal_thr * h->cal_thr : 0.f;
+    g.gate = h->cal_thr;
+    g.out_idx = (long long *)idx;
+    g.out_val = (float2 *)val;
+    g.rs = rs;
+    g.full_nb = (int)full_nb;
+    g.fire_list = h->fire_list;
+    g.fire_count = h->fire_count;
+    g.coarse_out = coarse_out;
+    band_gate_kernel<<<(batch + 7) / 8, 256, 0, s>>>(g);
+    CUDA_TRY(cudaGetLastError());
+  }
+  return MFB_OK;
+}
+
 static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t binsize,
                          float threshold, size_t start, size_t end, int64_t *idx, void *val,
                          int32_t *counts, int rs, int phase = 0, void *table = nullptr,
@@ -1070,6 +1155,9 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
     a.fire_count = h->fire_count;
     a.full_nb = (int)nb;
     CUDA_TRY(launch_flat<MODE_GATE>((int)h->m, *h->cc, a, s));
+  } else if (h->m == (size_t)BAND_BIG) {
+    r = band_big_coarse(h, d0, nd, t0, nt, cs, ce, idx, val, rs, nb, nullptr, s);
+    if (r) return r;
   } else {
     TcRunArgs a;
     memset(&a, 0, sizeof a);
@@ -1287,6 +1375,8 @@ extern "C" int mfb_hier_coarse_values(mfb_hplan *h, int d0, int nd, int t0, int 
     CUDA_TRY(launch_flat<MODE_GATE>((int)h->m, *h->cc, a, s));
     return MFB_OK;
   }
+  if (h->m == (size_t)BAND_BIG)
+    return band_big_coarse(h, d0, nd, t0, nt, cs, ce, nullptr, nullptr, 1, 0, out, s);
   TcRunArgs a;
   memset(&a, 0, sizeof a);
   a.data = h->full->data;

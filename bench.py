@@ -89,7 +89,7 @@ def parse():
                          "jobs in one persistent launch; large: n=262144 bank, flat and "
                          "hierarchical")
     ap.add_argument("--jobs", type=int, default=256, help="batched workload: number of jobs")
-    ap.add_argument("--large-coarse", default="fp32", choices=["fp32", "bf16x3", "fp16x3"],
+    ap.add_argument("--large-coarse", default="fp16x3", choices=["fp32", "bf16x3", "fp16x3"],
                     help="large workload: coarse arithmetic of the hierarchical filter")
     ap.add_argument("--no-tune", action="store_true", help="batched workload: default configs")
     ap.add_argument("--no-sub", action="store_true",
@@ -716,8 +716,8 @@ def sub_config3(args, dev, local, flush, peak):
 
 
 def sub_config4(args, dev, local, flush, peak):
-    rec = large_record(dev, local, args.seed, steps=3, warmup=2, coarse="fp32",
-                       cpu_sample=False)
+    rec = large_record(dev, local, args.seed, steps=3, warmup=2, coarse="fp16x3",
+                       cpu_sample=False, compare="fp32")
     rec.pop("clocks", None)
     return rec
 
@@ -911,24 +911,50 @@ def fp64_detections(D, H, thr):
     return det
 
 
-def large_record(dev, local, seed, steps, warmup, coarse, cpu_sample=True, rank=0):
+def large_record(dev, local, seed, steps, warmup, coarse, cpu_sample=True, rank=0,
+                 compare=None):
     """Config 4: the n = 262144 bank, flat and hierarchical, with the false
-    dismissal of both against an FP64 dense correlation."""
+    dismissal of both against an FP64 dense correlation; `compare` names
+    another coarse kind whose hierarchical run is timed beside it."""
     import torch
     import apogee_b200 as mf
-    from apogee_b200 import synthetic
+    from apogee_b200 import synthetic, _lib
     D, H, power, inj = synthetic.large_workload(LN, LND, LNT, seed=seed + 1000 * rank,
                                                 device=str(dev))
     gdev = "gpu:%d" % local
     flat = mf.MatchedFilter(LN, LND, LNT, device=gdev)
     flat.set_data(D)
     flat.set_templates(H)
-    hf = mf.HierarchicalFilter(LN, LND, LNT, snr=LSNR, fd=LFD, band=LBAND, device=gdev,
-                               coarse=coarse)
-    hf.set_reference(power.cpu().numpy())
-    hf.set_templates(H)
-    hf.set_data(D)
+
+    def make_hier(kind):
+        h = mf.HierarchicalFilter(LN, LND, LNT, snr=LSNR, fd=LFD, band=LBAND, device=gdev,
+                                  coarse=kind)
+        h.set_reference(power.cpu().numpy())
+        h.set_templates(H)
+        h.set_data(D)
+        return h
+    hf = make_hier(coarse)
     pairs = LND * LNT
+    L = _lib.lib()
+    nbl = LN // LBIN
+    pidx = torch.empty(pairs * nbl, dtype=torch.int64, device=dev)
+    pval = torch.empty(pairs * nbl, dtype=torch.complex64, device=dev)
+
+    def coarse_ms(h, reps=3):
+        """The coarse pass and gate alone (mfb_hier_run_phase 1), CUDA events."""
+        h.run_device(binsize=LBIN, threshold=LTHR)
+        tot = 0.0
+        for _ in range(reps):
+            h._bind_stream()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            _lib.check(L.mfb_hier_run_phase(h._hplan, 1, 0, LND, 0, LNT, LBIN, LTHR, 0, LN,
+                                            pidx.data_ptr(), pval.data_ptr(), None))
+            b.record()
+            torch.cuda.synchronize(dev)
+            tot += a.elapsed_time(b)
+        return tot / reps
 
     def timed(fn, steps, warm):
         for _ in range(warm):
@@ -959,7 +985,23 @@ def large_record(dev, local, seed, steps, warmup, coarse, cpu_sample=True, rank=
     missed_f = int((det & (fidx < 0)).sum().item())
     refine = hf.refine_rate
     gate = hf._coarse_value(LBAND)
-    del flat, hf
+    hier_coarse_ms = coarse_ms(hf)
+    other = None
+    if compare:
+        del hf
+        torch.cuda.empty_cache()
+        h2 = make_hier(compare)
+        h2_ms = timed(lambda: h2.run_device(binsize=LBIN, threshold=LTHR), steps,
+                      max(warmup, 2))
+        i2, _ = h2.run_device(binsize=LBIN, threshold=LTHR)
+        other = {"coarse": compare, "value": pairs / (h2_ms * 1e-3), "ms_per_step": h2_ms,
+                 "coarse_gate_ms": coarse_ms(h2), "refine_rate": h2.refine_rate,
+                 "speedup_vs_flat": flat_ms / h2_ms,
+                 "fp64_detections_missed": int((det & (i2 < 0)).sum().item())}
+        del h2
+    else:
+        del hf
+    del flat
     peak = fp32_peak(local)
     flops = FLOPS_PER_PAIR(LN) * pairs
     cb = None
@@ -995,7 +1037,9 @@ def large_record(dev, local, seed, steps, warmup, coarse, cpu_sample=True, rank=
         "flat": {"value": pairs / (flat_ms * 1e-3), "unit": "pairs/s", "ms_per_step": flat_ms,
                  "fp64_detections_missed": missed_f},
         "hier": {"value": pairs / (hier_ms * 1e-3), "ms_per_step": hier_ms, "coarse": coarse,
+                 "coarse_gate_ms": hier_coarse_ms,
                  "refine_rate": refine, "speedup_vs_flat": flat_ms / hier_ms},
+        "hier_other_coarse": other,
         "false_dismissal": {"fp64_detections": n_det, "missed": missed_h,
                             "rate": missed_h / n_det if n_det else 0.0, "injections": inj},
         "roofline_flat": {"bound": "fp32", "achieved": flops / (flat_ms * 1e-3) / 1e12,
@@ -1015,7 +1059,7 @@ def large_arm(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     rec = large_record(dev, local, args.seed, args.steps, args.warmup, args.large_coarse,
-                       rank=rank)
+                       rank=rank, compare="fp32" if args.large_coarse != "fp32" else None)
     if rank == 0:
         line = {"metric": LARGE_METRIC, "value": rec.pop("value"), "unit": "pairs/s",
                 "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,

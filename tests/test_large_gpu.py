@@ -113,3 +113,38 @@ def test_large_run_series(n):
         bad = parity.compare(idx[b:b + 1], val[b:b + 1], z[b:b + 1], bs, 0.0,
                              (int(ws[b]), int(we[b])))
         assert not bad, (b, bad[:3])
+
+
+@pytest.mark.parametrize("coarse", ["fp16x3", "bf16x3"])
+@pytest.mark.parametrize("nd,nt,window", [(3, 5, None), (4, 160, (1000, 30000))])
+def test_band_16384_tensor_core_coarse(coarse, nd, nt, window):
+    """The split-precision tensor-core coarse pass at band 16384 (a four-step
+    around the 512-point tensor-core pass, batches of 512 pairs): coarse
+    maxima against FP64 over the widened coarse window, and a gated run whose
+    fired rows are the flat filter's rows and whose dismissed rows are empty."""
+    import apogee_b200 as mf
+    n, band = 32768, 16384
+    rng = np.random.default_rng(nd * 1000 + nt)
+    D = (rng.standard_normal((nd, n)) + 1j * rng.standard_normal((nd, n))).astype(np.complex64)
+    H = (rng.standard_normal((nt, n)) + 1j * rng.standard_normal((nt, n))).astype(np.complex64)
+    hf = mf.HierarchicalFilter(n, nd, nt, band=band, coarse=coarse)
+    hf.set_coarse_threshold(0.0)
+    hf.set_data(D)
+    hf.set_templates(H)
+    cv = hf.coarse_values(window=window)
+    cm = oracle.coarse_max(D, H, band, None, window)
+    rel = np.abs(cv - cm) / cm
+    assert rel.max() < 2e-5, rel.max()
+    gate = float(np.quantile(cm, 0.7))
+    hf.set_coarse_threshold(gate)
+    bs = n // 16
+    out = hf.run(binsize=bs, threshold=0.0, window=window).copy()
+    flat = mf.MatchedFilter(n, nd, nt)
+    flat.set_data(D)
+    flat.set_templates(H)
+    ref = flat.run(binsize=bs, threshold=0.0, window=window)
+    fired = (out["index"] >= 0).any(-1)
+    assert hf.last_refinements == int(fired.sum())
+    np.testing.assert_array_equal(fired, cv >= gate)
+    np.testing.assert_array_equal(out[fired], ref[fired])
+    assert (out["index"][~fired] == -1).all() and (out["value"][~fired] == 0).all()
