@@ -190,6 +190,8 @@ flat2_kernel(const FlatArgs a) {
   const int t = threadIdx.x;
   const int lane = t & 31;
   const long long total = a.list ? (long long)(*a.list_count) : (long long)a.nd * a.nt;
+  if (a.list && a.trig_total && blockIdx.x == 0 && threadIdx.x == 0)
+    *a.trig_total += (unsigned long long)total;
   const long long items = (total + 1) / 2;
   const long long per = items / gridDim.x, extra = items % gridDim.x;
   const long long ibeg = blockIdx.x * per + (blockIdx.x < extra ? blockIdx.x : extra);

@@ -60,6 +60,9 @@ struct FlatArgs {
   int full_nb;                // bins of the full-size output written as (-1,0) when dismissed
   float *coarse_out;          // if set: write max |z| over the window per row instead of gating
   int data_cg;                // 1: data rows were written in this launch (coherent loads)
+  // listed mode: if set, the launch adds the row count to this running total
+  // (the hierarchical plan's trigger count) -- one thread, once
+  unsigned long long *trig_total;
 };
 
 template <int N>
@@ -771,6 +774,7 @@ rows_kernel(const FlatArgs a) {
   using Geo = FlatGeo<N>;
   extern __shared__ __align__(16) float2 smem[];
   const long long total = *a.list_count;
+  if (a.trig_total && blockIdx.x == 0 && threadIdx.x == 0) *a.trig_total += (unsigned long long)total;
   const long long items = (total + Geo::G - 1) / Geo::G;
   const long long per = items / gridDim.x, extra = items % gridDim.x;
   const long long ibeg = blockIdx.x * per + (blockIdx.x < extra ? blockIdx.x : extra);

@@ -611,10 +611,13 @@ extern "C" int mfb_run_records(mfb_plan *p, int d0, int nd, int t0, int nt, size
                   (char *)records + 8, counts, 2);
 }
 
+// trig_total: if set, the listed launch adds the row count to it on the
+// device (the large-n path leaves it to the caller: returns 1 in *added = 0).
 static int run_rows_impl(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *rows,
                          const int32_t *nrows, int max_rows, size_t binsize, float threshold,
                          size_t start, size_t end, int64_t *idx, void *val, int32_t *counts,
-                         int rs) {
+                         int rs, unsigned long long *trig_total = nullptr, bool *added = nullptr) {
+  if (added) *added = false;
   if (!p) return fail(MFB_ERR_ARG, "null plan");
   size_t nb;
   int r = check_run(p, d0, nd, t0, nt, binsize, start, end, &nb);
@@ -638,10 +641,12 @@ static int run_rows_impl(mfb_plan *p, int d0, int nd, int t0, int nt, const int3
     return run_large(p, d0, nd, t0, nt, rows, cnt, binsize, threshold, start, end, nb, idx, val,
                      counts, rs);
   }
+  a.trig_total = trig_total;
   if (p->packed && flat2_applies((int)p->n, *p->c, a))
     CUDA_TRY(launch_flat2(*p->c, a, p->stream));
   else
     CUDA_TRY(launch_rows((int)p->n, *p->c, a, p->stream));
+  if (added) *added = trig_total != nullptr;
   return MFB_OK;
 }
 
@@ -1181,8 +1186,9 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
   if (phase == 1) return MFB_OK;
   if (join) CUDA_TRY(cudaStreamWaitEvent(s, h->ev_join, 0));
   // Refine the survivors with the full filter; no host decision in between.
+  bool counted = false;
   r = run_rows_impl(p, d0, nd, t0, nt, h->fire_list, h->fire_count, nd * nt, binsize, threshold,
-                    start, end, idx, val, counts, rs);
+                    start, end, idx, val, counts, rs, table ? nullptr : h->trig_total, &counted);
   if (r) return r;
   if (table) {
     // table, info: device-visible pointers of the caller's pinned host memory
@@ -1216,7 +1222,7 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
     h->host_table = table;
     h->host_rows = rows;
     h->host_nb = (long long)nb;
-  } else {
+  } else if (!counted) {
     accumulate_triggers<<<1, 1, 0, s>>>(h->fire_count, h->trig_total);
     CUDA_TRY(cudaGetLastError());
   }
