@@ -883,8 +883,12 @@ class HierarchicalFilter(MatchedFilter):
         The default structured table is kept in pinned host memory between
         calls and only the refined rows cross the host link (every row the
         gate dismisses is all empty records), written by the device straight
-        into the host table: it is returned read-only and is updated in place
-        by the next call.
+        into the host table.  As in the reference ("Results may reuse
+        buffers ... The next run on this filter overwrites it in place;
+        .copy() anything that must outlive that call",
+        python/matchedfilter/__init__.py:463-466), the next call updates it in
+        place; it is returned read-only because the device tracks which of its
+        rows hold refined results.
         """
         binsize, start, end, d0, nd, t0, nt, nb = self._run_args(binsize, window, data, templates)
         threshold = float(threshold)
