@@ -511,10 +511,13 @@ static FlatArgs base_args(const mfb_plan *p, int d0, int nd, int t0, int nt, siz
 
 // Two-pass path for n > 16384.  list/nlist: listed output rows (host count),
 // or nullptr for the dense block.  Scratch is allocated on first use.
+#ifndef MFB_LARGE_SCRATCH_MB
+#define MFB_LARGE_SCRATCH_MB 64
+#endif
 static int large_scratch(mfb_plan *p) {
   if (!p->lY) {
     const size_t per = p->n * sizeof(float2);
-    int b = (int)std::max<size_t>(1, ((size_t)64 << 20) / per);
+    int b = (int)std::max<size_t>(1, ((size_t)MFB_LARGE_SCRATCH_MB << 20) / per);
     CUDA_TRY(cudaMalloc(&p->lY, (size_t)b * per));
     CUDA_TRY(cudaMalloc(&p->lrec, (size_t)b * LARGE_MAX_BINS * sizeof(uint4)));
     p->lbatch = b;
