@@ -324,6 +324,10 @@ flat2_kernel(const FlatArgs a) {
         const long long o = row * nb + b;
         a.out_idx[o * a.rs] = ix;
         a.out_val[o * a.rs] = val;
+        if (a.host_rec)   // 16-byte store over the host link into the host table
+          a.host_rec[o] = make_int4((int)(unsigned)(unsigned long long)ix,
+                                    (int)(unsigned)((unsigned long long)ix >> 32),
+                                    __float_as_int(val.x), __float_as_int(val.y));
         if (a.out_cnt && kk != 0ull) atomicAdd(a.out_cnt + row, 1);
       }
       // clear the other parity's keys for the next item (not read before the

@@ -63,6 +63,9 @@ struct FlatArgs {
   // listed mode: if set, the launch adds the row count to this running total
   // (the hierarchical plan's trigger count) -- one thread, once
   unsigned long long *trig_total;
+  // if set (record output, rs == 2): every output record is also stored here,
+  // the caller's pinned host table seen from the device (flat2_kernel only)
+  int4 *host_rec;
 };
 
 template <int N>

@@ -76,13 +76,17 @@ inline cudaError_t launch_hier_scale(const HierScaleArgs &a, cudaStream_t s) {
 // dismisses is all empty records (index -1, value 0), so when the host table
 // holds the previous run's result only the rows that change cross the link:
 // the rows refined now are written, and the rows refined last time but not
-// now are reset to empty.  Two launches in stream order:
-//   hier_write_kernel    writes the rows of this run's list and marks them
-//                        (bit p of mark[row], p the run's parity);
+// now are reset to empty.  Three launches:
+//   hier_mark_kernel     marks the rows of this run's list (bit p of
+//                        mark[row], p the run's parity), after the coarse pass;
 //   hier_unwrite_kernel  resets the rows of the previous list that carry no
 //                        mark of this run, clears the previous run's mark bit,
 //                        stores this run's list for the next one (list store
-//                        p) and, in its last block, flips the parity.
+//                        p) and, in its last block, flips the parity -- these
+//                        two on a second stream while the refine runs (the
+//                        rows they touch are not the refined ones);
+//   hier_write_kernel    writes the refined rows after the refine, unless the
+//                        refine kernel stored them into the table itself.
 // State on the device (so that a CUDA graph of the run replays correctly):
 // mark[rows], list_store[2][rows], count_store[2], ctl = {parity, blocks
 // done, rows reset}.
@@ -102,12 +106,23 @@ struct HierHostArgs {
   long long full_bytes;       // bytes of that whole copy
 };
 
-static __global__ void hier_write_kernel(const HierHostArgs a) {
+// Marks this run's rows (bit p of mark[row]); runs before hier_unwrite_kernel,
+// which needs the marks, and may run beside the refine: neither reads the
+// refined values.
+static __global__ void hier_mark_kernel(const HierHostArgs a) {
   const long long c = *a.count;
   const uint32_t bit = 1u << (a.ctl[0] & 1u);
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   for (long long i = t0; i < c; i += stride) a.mark[a.list[i]] |= bit;   // rows are unique
+}
+
+// Copies this run's refined rows into the host table (after the refine;
+// not needed when the refine kernel stored them there itself).
+static __global__ void hier_write_kernel(const HierHostArgs a) {
+  const long long c = *a.count;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (a.write_rows)
     for (long long e = t0; e < c * a.nb; e += stride) {
       const long long i = e / a.nb;

@@ -619,8 +619,10 @@ extern "C" int mfb_run_records(mfb_plan *p, int d0, int nd, int t0, int nt, size
 static int run_rows_impl(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *rows,
                          const int32_t *nrows, int max_rows, size_t binsize, float threshold,
                          size_t start, size_t end, int64_t *idx, void *val, int32_t *counts,
-                         int rs, unsigned long long *trig_total = nullptr, bool *added = nullptr) {
+                         int rs, unsigned long long *trig_total = nullptr, bool *added = nullptr,
+                         int4 *host_rec = nullptr, bool *host_written = nullptr) {
   if (added) *added = false;
+  if (host_written) *host_written = false;
   if (!p) return fail(MFB_ERR_ARG, "null plan");
   size_t nb;
   int r = check_run(p, d0, nd, t0, nt, binsize, start, end, &nb);
@@ -645,10 +647,15 @@ static int run_rows_impl(mfb_plan *p, int d0, int nd, int t0, int nt, const int3
                      counts, rs);
   }
   a.trig_total = trig_total;
-  if (p->packed && flat2_applies((int)p->n, *p->c, a))
+  if (p->packed && flat2_applies((int)p->n, *p->c, a)) {
+    if (host_rec && rs == 2) {
+      a.host_rec = host_rec;
+      if (host_written) *host_written = true;
+    }
     CUDA_TRY(launch_flat2(*p->c, a, p->stream));
-  else
+  } else {
     CUDA_TRY(launch_rows((int)p->n, *p->c, a, p->stream));
+  }
   if (added) *added = trig_total != nullptr;
   return MFB_OK;
 }
@@ -806,6 +813,9 @@ struct mfb_hplan {
   // a second stream while the coarse pass runs
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // mfb_hier_run_host: the host-table bookkeeping runs on `side` beside the
+  // refine, from ev_coarse (coarse pass done) to ev_table
+  cudaEvent_t ev_coarse = nullptr, ev_table = nullptr;
   // mfb_hier_run_host repeated with identical arguments replays one CUDA
   // graph of the whole run (captured on `cap` at the second such call)
   struct RunKey {
@@ -863,6 +873,8 @@ extern "C" int mfb_hier_create(mfb_hplan **out, size_t n, int ndata, int ntmpl, 
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_coarse, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_table, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMemset(h->trig_total, 0, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(h->ct, 0, (size_t)ntmpl * band * sizeof(float2));
@@ -924,6 +936,8 @@ extern "C" int mfb_hier_destroy(mfb_hplan *h) {
   if (h->side) cudaStreamDestroy(h->side);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->ev_coarse) cudaEventDestroy(h->ev_coarse);
+  if (h->ev_table) cudaEventDestroy(h->ev_table);
   if (h->graph) cudaGraphExecDestroy(h->graph);
   if (h->cap) cudaStreamDestroy(h->cap);
   free(h->tready);
@@ -1187,16 +1201,14 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
   }
   }
   if (phase == 1) return MFB_OK;
-  if (join) CUDA_TRY(cudaStreamWaitEvent(s, h->ev_join, 0));
-  // Refine the survivors with the full filter; no host decision in between.
-  bool counted = false;
-  r = run_rows_impl(p, d0, nd, t0, nt, h->fire_list, h->fire_count, nd * nt, binsize, threshold,
-                    start, end, idx, val, counts, rs, table ? nullptr : h->trig_total, &counted);
-  if (r) return r;
+  // Host table: its bookkeeping (marks of this run's rows, reset of the
+  // previous run's rows that are not refined now, list store, parity) needs
+  // only the survivor list, so it runs on the second stream beside the refine.
+  HierHostArgs ha;
+  bool same = false;
+  int hgrid = 1;
+  const long long hrows = (long long)nd * nt;
   if (table) {
-    // table, info: device-visible pointers of the caller's pinned host memory
-    const long long rows = (long long)nd * nt;
-    HierHostArgs ha;
     ha.records = (const int4 *)idx;
     ha.table = (int4 *)table;
     ha.nb = (long long)nb;
@@ -1209,21 +1221,38 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
     ha.rows = (long long)h->nd * h->nt;
     ha.total = h->trig_total;
     ha.info = info;
-    ha.full_bytes = rows * (long long)nb * 16;
-    const bool same = table == h->host_table && rows == h->host_rows && (long long)nb == h->host_nb;
+    ha.full_bytes = hrows * (long long)nb * 16;
+    same = table == h->host_table && hrows == h->host_rows && (long long)nb == h->host_nb;
     ha.write_rows = same ? 1 : 0;
     int sms = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-    const int grid = hier_host_grid(rows * (long long)nb, sms);
+    hgrid = hier_host_grid(hrows * (long long)nb, sms);
+    CUDA_TRY(cudaEventRecord(h->ev_coarse, s));
+    CUDA_TRY(cudaStreamWaitEvent(h->side, h->ev_coarse, 0));
+    hier_mark_kernel<<<hgrid, 256, 0, h->side>>>(ha);
+    CUDA_TRY(cudaGetLastError());
+    hier_unwrite_kernel<<<hgrid, 256, 0, h->side>>>(ha);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(h->ev_table, h->side));
+  }
+  if (join) CUDA_TRY(cudaStreamWaitEvent(s, h->ev_join, 0));
+  // Refine the survivors with the full filter; no host decision in between.
+  // With the host table as it was left by this plan, the packed kernel also
+  // stores the refined rows into it.
+  bool counted = false, host_written = false;
+  r = run_rows_impl(p, d0, nd, t0, nt, h->fire_list, h->fire_count, nd * nt, binsize, threshold,
+                    start, end, idx, val, counts, rs, table ? nullptr : h->trig_total, &counted,
+                    table && same ? (int4 *)table : nullptr, &host_written);
+  if (r) return r;
+  if (table) {
     if (!same) CUDA_TRY(cudaMemcpyAsync(table, idx, (size_t)ha.full_bytes, cudaMemcpyDefault, s));
-    // this run's rows (and their marks), then the previous run's rows that
-    // no longer hold a refined row
-    hier_write_kernel<<<grid, 256, 0, s>>>(ha);
-    CUDA_TRY(cudaGetLastError());
-    hier_unwrite_kernel<<<grid, 256, 0, s>>>(ha);
-    CUDA_TRY(cudaGetLastError());
+    else if (!host_written) {
+      hier_write_kernel<<<hgrid, 256, 0, s>>>(ha);
+      CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaStreamWaitEvent(s, h->ev_table, 0));
     h->host_table = table;
-    h->host_rows = rows;
+    h->host_rows = hrows;
     h->host_nb = (long long)nb;
   } else if (!counted) {
     accumulate_triggers<<<1, 1, 0, s>>>(h->fire_count, h->trig_total);
