@@ -2,6 +2,7 @@
 // template scaling (src/hmf.c:118-156), plus the interface of the tensor-core
 // coarse pass (coarse_tc.cu).
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -177,6 +178,23 @@ static __global__ void hier_unwrite_kernel(const HierHostArgs a) {
       __threadfence();
       a.ctl[0] = q;                                    // the next run's parity
     }
+  }
+}
+
+// The lowest `cols` bins (as 8-byte complex values) of `rows` data rows read
+// straight from pinned, mapped host memory by the device: many 8- or 16-byte
+// reads in flight at once, where a strided copy would move the 16 short rows
+// one after another.  VEC = 2: 16-byte accesses (src 16-byte aligned).
+template <int VEC>
+static __global__ void band_gather_kernel(float2 *dst, long long dst_row, const float2 *src,
+                                          long long src_row, int cols, int rows) {
+  using V = typename std::conditional<VEC == 2, float4, float2>::type;
+  const int cv = cols / VEC;
+  const long long total = (long long)rows * cv;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / cv), c = (int)(i - (long long)r * cv);
+    reinterpret_cast<V *>(dst + r * dst_row)[c] = reinterpret_cast<const V *>(src + r * src_row)[c];
   }
 }
 

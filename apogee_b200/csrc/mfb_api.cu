@@ -1144,10 +1144,31 @@ static int hier_run_impl(mfb_hplan *h, int d0, int nd, int t0, int nt, size_t bi
   bool join = false;
   if (data_host && phase == 0) {
     // all data rows from host memory: the band the coarse pass reads first,
-    // the rest on the side stream, joined before the refine
+    // the rest on the side stream, joined before the refine.  From pinned
+    // memory the device gathers the band itself (one short launch instead of
+    // a copy of nd strided rows); pageable memory takes the copy.
     const size_t row = h->n * sizeof(float2), band = h->m * sizeof(float2);
-    CUDA_TRY(cudaMemcpy2DAsync(p->data, row, data_host, row, band, (size_t)h->nd,
-                               cudaMemcpyDefault, s));
+    cudaPointerAttributes pa;
+    const bool mapped = cudaPointerGetAttributes(&pa, data_host) == cudaSuccess &&
+                        pa.type == cudaMemoryTypeHost && pa.devicePointer != nullptr;
+    if (!mapped) cudaGetLastError();
+    if (mapped) {
+      const float2 *src = (const float2 *)pa.devicePointer;
+      const int elems = h->nd * (int)h->m;
+      if ((((uintptr_t)src) & 15) == 0) {
+        const int grid = std::max(1, std::min(1024, elems / 2 / 256));
+        band_gather_kernel<2><<<grid, 256, 0, s>>>(p->data, (long long)h->n, src, (long long)h->n,
+                                                   (int)h->m, h->nd);
+      } else {
+        const int grid = std::max(1, std::min(1024, elems / 256));
+        band_gather_kernel<1><<<grid, 256, 0, s>>>(p->data, (long long)h->n, src, (long long)h->n,
+                                                   (int)h->m, h->nd);
+      }
+      CUDA_TRY(cudaGetLastError());
+    } else {
+      CUDA_TRY(cudaMemcpy2DAsync(p->data, row, data_host, row, band, (size_t)h->nd,
+                                 cudaMemcpyDefault, s));
+    }
     CUDA_TRY(cudaEventRecord(h->ev_fork, s));
     CUDA_TRY(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
     CUDA_TRY(cudaMemcpy2DAsync((char *)p->data + band, row, (const char *)data_host + band, row,
