@@ -90,3 +90,38 @@ def test_costmodel_candidates_and_pick():
     assert costmodel.pick({256: 30.0, 512: 30.0}) == 512
     with pytest.raises(ValueError):
         costmodel.pick({})
+
+
+def test_coarse_kind_auto_and_tensor_core_bands():
+    """coarse="auto" takes the BF16 split tensor-core pass at the bands where
+    it is the faster (AUTO_TC_BANDS) and the FP32 pass elsewhere; the explicit
+    tensor-core kinds cover TC_BANDS only."""
+    import apogee_b200 as mf
+    from apogee_b200 import _lib
+    assert mf.AUTO_TC_BANDS <= mf.TC_BANDS
+    assert mf._coarse_kind("auto", 512) == _lib.COARSE_BF16X3
+    assert mf._coarse_kind("auto", 16384) == _lib.COARSE_FP32
+    assert mf._coarse_kind("auto", 1024) == _lib.COARSE_FP32
+    assert mf._coarse_kind("auto") is None
+    assert mf._coarse_kind("fp16x3", 16384) == _lib.COARSE_FP16X3
+    import pytest
+    with pytest.raises(ValueError):
+        mf._coarse_kind("tf32")
+
+
+def test_large_workload_subsample_is_the_full_banks_draws():
+    """A materialised subsample of the large-bank generator has the full
+    bank's data, profile and injections (CPU torch)."""
+    import numpy as np
+    import torch
+    from apogee_b200 import synthetic
+    n, nt = 1024, 12
+    D1, H1, p1, inj1 = synthetic.large_workload(n, 3, nt, seed=4, device="cpu", chunk=5)
+    D2, H2, p2, inj2 = synthetic.large_workload(n, 3, nt, seed=4, device="cpu", chunk=5,
+                                                materialize=[2, 7, 11])
+    assert inj1 == inj2
+    torch.testing.assert_close(D1, D2)
+    torch.testing.assert_close(p1, p2)
+    torch.testing.assert_close(H1[[2, 7, 11]], H2)
+    assert np.isclose(float(p1.sum()) * n / n, float((H1.abs().double() ** 2).mean(0).sum()),
+                      rtol=1e-6)
