@@ -394,12 +394,12 @@ struct mfb_plan {
 };
 
 struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
+  int prev = -1, dev_;
+  explicit DeviceGuard(int dev) : dev_(dev) {
     if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
     if (prev != dev) cudaSetDevice(dev);
   }
-  ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+  ~DeviceGuard() { if (prev >= 0 && prev != dev_) cudaSetDevice(prev); }
 };
 
 extern "C" int mfb_create(mfb_plan **out, size_t n, int ndata, int ntmpl, int device) {
