@@ -70,6 +70,7 @@ SIGNATURES = {
     "mfb_destroy": (_I, [_P]),
     "mfb_set_stream": (_I, [_P, _P]),
     "mfb_set_packed": (_I, [_P, _I]),
+    "mfb_set_cluster": (_I, [_P, _I]),
     "mfb_set_data": (_I, [_P, _I, _I, _P]),
     "mfb_set_templates": (_I, [_P, _I, _I, _P]),
     "mfb_run": (_I, [_P, _I, _I, _I, _I, _SZ, _F, _SZ, _SZ, _P, _P, _P]),
@@ -84,6 +85,7 @@ SIGNATURES = {
     "mfb_hier_destroy": (_I, [_P]),
     "mfb_hier_set_stream": (_I, [_P, _P]),
     "mfb_hier_set_packed": (_I, [_P, _I]),
+    "mfb_hier_set_cluster": (_I, [_P, _I]),
     "mfb_hier_set_data": (_I, [_P, _I, _I, _P]),
     "mfb_hier_set_templates": (_I, [_P, _I, _I, _P]),
     "mfb_hier_set_reference": (_I, [_P, _P]),

@@ -41,6 +41,7 @@ struct LargeArgs {
   int n, N1, N2;
   int d0, nd, t0, nt;                   // pair block; output row = (d-d0)*nt + (t-t0)
   const int32_t *list;                  // listed output rows, or nullptr (dense block)
+  const int32_t *list_count;            // cluster kernel: the list's length on the device
   long long total;                      // pairs in the dense block or the list
   long long pair0;                      // first pair of this batch
   int batch;                            // pairs in this batch

@@ -25,6 +25,7 @@
 #include "hier_kernels.cuh"
 #include "band_kernels.cuh"
 #include "large_kernel.cuh"
+#include "cluster_kernel.cuh"
 #include "adjoint_kernel.cuh"
 #include "batch_kernel.cuh"
 #include "gate_kernels.cuh"
@@ -240,12 +241,18 @@ static bool is_large(size_t n) { return n > 16384; }
 // ------------------------------------------------------------ large-n setup
 // n = N1 * N2 with N2 = 2^ceil(log2(n)/2) (<= 1024, the pass-A CTA size; two
 // pass-A CTAs per SM at N2 = 512).
+struct ClusterCfg {
+  int C = 0, clusters = 0, clusters_small = 0, smem = 0;   // small: at most LARGE_SMALL_BINS bins
+};
 struct LargeConst {
   int N1 = 0, N2 = 0, lo_bits = 0;
   float2 *tw_hi = nullptr, *tw_lo = nullptr;
   NConst *c1 = nullptr, *c2 = nullptr;
   int grid_a = 0, grid_b = 0, smem_a = 0, smem_b = 0, cta_a = 0, cta_b = 0;
   int grid_bs = 0, smem_bs = 0;   // pass B with at most LARGE_SMALL_BINS keys
+  // n = 32768 / 65536: one thread-block cluster per pair (cluster_kernel);
+  // cl[0]: 256-thread CTAs, cl[1]: 512-thread CTAs
+  ClusterCfg cl[2];
 };
 static std::map<std::pair<int, int>, LargeConst> g_large;
 
@@ -276,6 +283,71 @@ static int large_b_attr(LargeConst &c, int sms) {
   c.grid_b = b * sms;
   c.grid_bs = bs * sms;
   return MFB_OK;
+}
+
+template <int N1, int N2, int C>
+static void cluster_config(cudaLaunchConfig_t &cfg, cudaLaunchAttribute *at, int clusters,
+                           int smem, cudaStream_t s) {
+  cfg = cudaLaunchConfig_t{};
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(C * clusters);
+  cfg.blockDim = dim3(ClusterGeo<N1, N2, C>::TH);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+}
+
+// Cluster kernel set-up for one geometry: shared memory, the non-portable
+// cluster size 16 where it is used, and how many clusters fit at once.
+template <int N1, int N2, int C>
+static int cluster_attr(ClusterCfg &k) {
+  using Geo = ClusterGeo<N1, N2, C>;
+  k.smem = Geo::SMEM_FIXED + LARGE_MAX_BINS * 8;
+  CUDA_TRY(cudaFuncSetAttribute(cluster_kernel<N1, N2, C>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem));
+  if (C > 8)
+    CUDA_TRY(cudaFuncSetAttribute(cluster_kernel<N1, N2, C>,
+                                  cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute at[1];
+  cluster_config<N1, N2, C>(cfg, at, 64, k.smem, nullptr);
+  int n = 0, ns = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveClusters(&n, cluster_kernel<N1, N2, C>, &cfg));
+  cluster_config<N1, N2, C>(cfg, at, 64, Geo::SMEM_FIXED + LARGE_SMALL_BINS * 8, nullptr);
+  CUDA_TRY(cudaOccupancyMaxActiveClusters(&ns, cluster_kernel<N1, N2, C>, &cfg));
+  if (n < 1 || ns < 1) return fail(MFB_ERR_CUDA, "no cluster of %d CTAs fits for n=%d", C, N1 * N2);
+  k.C = C;
+  k.clusters = n;
+  k.clusters_small = ns;
+  return MFB_OK;
+}
+
+template <int N1, int N2, int C>
+static cudaError_t launch_cluster_t(const LargeArgs &a, int clusters, int smem, cudaStream_t s) {
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute at[1];
+  cluster_config<N1, N2, C>(cfg, at, clusters, smem, s);
+  return cudaLaunchKernelEx(&cfg, cluster_kernel<N1, N2, C>, a);
+}
+
+// One launch for every pair of the block or the list (no scratch, no host
+// decision).  dense_pairs bounds the cluster count when the pairs are known.
+static cudaError_t launch_cluster(const LargeConst &c, int mode, const LargeArgs &a,
+                                  long long dense_pairs, cudaStream_t s) {
+  const ClusterCfg &k = c.cl[mode - 1];
+  const bool few = a.nb <= LARGE_SMALL_BINS;
+  long long m = few ? k.clusters_small : k.clusters;
+  if (dense_pairs > 0) m = std::min(m, dense_pairs);
+  const int smem = k.smem - (LARGE_MAX_BINS - (few ? LARGE_SMALL_BINS : a.nb)) * 8;
+  if (c.N1 == 128)
+    return mode == 1 ? launch_cluster_t<128, 256, 8>(a, (int)m, smem, s)
+                     : launch_cluster_t<128, 256, 4>(a, (int)m, smem, s);
+  return mode == 1 ? launch_cluster_t<256, 256, 16>(a, (int)m, smem, s)
+                   : launch_cluster_t<256, 256, 8>(a, (int)m, smem, s);
 }
 
 static int get_large(int device, int n, LargeConst **out) {
@@ -315,6 +387,14 @@ static int get_large(int device, int n, LargeConst **out) {
     case 512: r = large_b_attr<512>(c, sms); break;
     case 1024: r = large_b_attr<1024>(c, sms); break;
     default: return fail(MFB_ERR_UNSUPPORTED, "no four-step split for n=%d", n);
+  }
+  if (r) return r;
+  if (n == 32768) {
+    r = cluster_attr<128, 256, 8>(c.cl[0]);
+    if (r == MFB_OK) r = cluster_attr<128, 256, 4>(c.cl[1]);
+  } else if (n == 65536) {
+    r = cluster_attr<256, 256, 16>(c.cl[0]);
+    if (r == MFB_OK) r = cluster_attr<256, 256, 8>(c.cl[1]);
   }
   if (r) return r;
   std::lock_guard<std::mutex> lk(g_const_mu);
@@ -391,6 +471,7 @@ struct mfb_plan {
   uint4 *lrec = nullptr;
   int lbatch = 0;
   int packed = 1;           // use flat2_kernel where it applies (mfb_set_packed)
+  int cluster = 0;          // cluster_kernel geometry where it applies (mfb_set_cluster)
 };
 
 struct DeviceGuard {
@@ -526,15 +607,24 @@ static int large_scratch(mfb_plan *p) {
 }
 
 // data: the rows to filter (default the plan's data rows).
+static bool cluster_applies(const mfb_plan *p) {
+  return p->cluster > 0 && p->lc && p->lc->cl[p->cluster - 1].C > 0;
+}
+
+// list: listed rows, nlist of them (counted on the host for the two-pass
+// batches), or list_count on the device (the cluster kernel reads it itself).
 static int run_large(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *list,
                      long long nlist, size_t binsize, float threshold, size_t start, size_t end,
                      size_t nb, int64_t *idx, void *val, int32_t *counts, int rs,
-                     const float2 *data = nullptr) {
+                     const float2 *data = nullptr, const int32_t *list_count = nullptr) {
   if (nb > (size_t)LARGE_MAX_BINS)
     return fail(MFB_ERR_UNSUPPORTED, "n=%zu supports at most %d bins per pair", p->n, LARGE_MAX_BINS);
   const LargeConst &c = *p->lc;
-  int sr = large_scratch(p);
-  if (sr) return sr;
+  const bool cl = cluster_applies(p) && (!list || list_count);
+  if (!cl) {
+    int sr = large_scratch(p);
+    if (sr) return sr;
+  }
   if (end > p->n) end = p->n;
   LargeArgs a;
   memset(&a, 0, sizeof a);
@@ -559,6 +649,11 @@ static int run_large(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t 
   a.out_val = (float2 *)val;
   a.rs = rs;
   a.out_cnt = counts;
+  if (cl) {
+    a.list_count = list ? list_count : nullptr;
+    CUDA_TRY(launch_cluster(c, p->cluster, a, list ? 0 : a.total, p->stream));
+    return MFB_OK;
+  }
   for (long long p0 = 0; p0 < a.total; p0 += p->lbatch) {
     a.pair0 = p0;
     a.batch = (int)std::min<long long>(p->lbatch, a.total - p0);
@@ -591,6 +686,13 @@ static int run_impl(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
     CUDA_TRY(launch_flat2(*p->c, a, p->stream));
   else
     CUDA_TRY(launch_flat<MODE_PEAKS>((int)p->n, *p->c, a, p->stream));
+  return MFB_OK;
+}
+
+extern "C" int mfb_set_cluster(mfb_plan *p, int mode) {
+  if (!p) return fail(MFB_ERR_ARG, "null plan");
+  if (mode < 0 || mode > 2) return fail(MFB_ERR_ARG, "cluster mode must be 0, 1 or 2");
+  p->cluster = mode;
   return MFB_OK;
 }
 
@@ -637,6 +739,11 @@ static int run_rows_impl(mfb_plan *p, int d0, int nd, int t0, int nt, const int3
   a.out_val = (float2 *)val;
   a.rs = rs;
   a.out_cnt = counts;   // rows not listed keep whatever the caller put there
+  if (is_large(p->n) && cluster_applies(p)) {
+    if (added) *added = false;
+    return run_large(p, d0, nd, t0, nt, rows, 0, binsize, threshold, start, end, nb, idx, val,
+                     counts, rs, nullptr, nrows);
+  }
   if (is_large(p->n)) {
     // the two-pass path sizes its batches on the host: read the row count
     int32_t cnt = 0;
@@ -967,6 +1074,12 @@ extern "C" int mfb_hier_set_packed(mfb_hplan *h, int on) {
   if (!h) return fail(MFB_ERR_ARG, "null plan");
   hier_drop_graph(h);
   return mfb_set_packed(h->full, on);
+}
+
+extern "C" int mfb_hier_set_cluster(mfb_hplan *h, int mode) {
+  if (!h) return fail(MFB_ERR_ARG, "null plan");
+  hier_drop_graph(h);
+  return mfb_set_cluster(h->full, mode);
 }
 
 extern "C" int mfb_hier_set_stream(mfb_hplan *h, void *stream) {
@@ -1334,7 +1447,7 @@ extern "C" int mfb_hier_run_host(mfb_hplan *h, int d0, int nd, int t0, int nt, s
   // A graph may hold copies from pinned host memory only (a pageable copy is
   // synchronous and cannot be captured), and the two-pass large-n refine
   // sizes its batches on the host.
-  bool graphable = !is_large(h->n);
+  bool graphable = !is_large(h->n) || cluster_applies(h->full);
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(h->full->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
     cudaGetLastError();
