@@ -367,3 +367,51 @@ def test_kept_results_follow_the_reuse_contract():
                               oracle.correlate(D1, H), bs)
     np.testing.assert_array_equal(first, second)          # the reused table
     assert not (first_copy["index"] == second["index"]).all()
+
+
+def test_repeated_run_skips_set_up_but_follows_every_change():
+    """A run() with the arguments of the previous one and a bank held in
+    place takes the short path (no argument checks or plan set-up); every
+    change in between -- the bank refilled in place, another binsize or
+    threshold, one data row set, new templates, a new gate -- is still seen."""
+    import torch
+    n, nd, nt, band = 4096, 4, 64, 512
+    rng = np.random.default_rng(31)
+    H = noise(rng, (nt, n))
+    hf = _filter(n, nd, nt, band, "bf16x3", 0.0)
+    hf.set_templates(H)
+    bank = torch.empty((nd, n), dtype=torch.complex64, pin_memory=True).numpy()
+    bank[:] = noise(rng, (nd, n))
+    hf.set_data(bank)
+    hf.set_coarse_threshold(float(np.quantile(hf.coarse_values(), 0.8)))
+
+    def check(**kw):
+        tab = hf.run(**kw).copy()
+        assert hf._repeat is not None
+        idx, val = _dense(hf, **kw)
+        np.testing.assert_array_equal(tab["index"], idx)
+        np.testing.assert_array_equal(tab["value"], val)
+        return tab
+
+    kw = dict(binsize=256, threshold=0.0)
+    check(**kw)
+    for step in range(3):
+        bank[:] = noise(rng, (nd, n))
+        bank[step % nd] += (50 * H[7 * step + 1].astype(np.complex128) *
+                            np.exp(-2j * np.pi * np.arange(n) * (100 + step) / n)).astype(np.complex64)
+        hf.set_data(bank)                      # the same array: refilled in place
+        tab = check(**kw)
+        assert tab["index"][step % nd, 7 * step + 1, 0] == 100 + step
+    check(binsize=512, threshold=0.0)
+    check(binsize=512, threshold=20.0)
+    hf.set_data(noise(rng, n), index=2)        # one row: the bank goes to the device mirror
+    check(binsize=512, threshold=20.0)
+    hf.set_templates(noise(rng, (nt, n)))
+    check(binsize=512, threshold=20.0)
+    hf.set_coarse_threshold(0.0)               # every pair refined
+    tab = check(binsize=512, threshold=20.0)
+    assert (tab["index"] >= 0).any()
+    bank[:] = noise(rng, (nd, n))
+    hf.set_data(bank)
+    check(binsize=512, threshold=20.0)
+    check(binsize=512, threshold=20.0, window=(0, n))    # a tuple window: same result
