@@ -324,7 +324,7 @@ __device__ __noinline__ void b_unit(int jid, int segi, int u, float2 *smem) {
     const float m2 = fmaf(v[q].x, v[q].x, v[q].y * v[q].y);
     if (lag >= j.ws && lag < j.we && m2 > j.t2) {
       const int bin = bin_of(lag - j.ws, j.binsize, inv_bs);
-      atomicMax(keys + bin, ((unsigned long long)__float_as_uint(m2) << 32) | (unsigned)(~lag));
+      atomicMax(keys + bin, ((unsigned long long)(__float_as_uint(m2) & ~31u) << 32) | (unsigned)(~lag));
       buf[pad16(k1)] = make_float2(v[q].x, v[q].y);
     }
   }

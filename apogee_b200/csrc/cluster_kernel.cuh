@@ -16,7 +16,7 @@
 //            of the CTA that owns row k2 (rows [r N2/C, (r+1) N2/C) belong to
 //            CTA r; a half-warp's 16 stores are one 128-byte row segment);
 //   pass B   each CTA runs the N1-point inverse FFTs of its rows, keeps the
-//            per-bin maximum of (|z|^2 bits << 32 | ~lag) with shared atomics
+//            per-bin maximum of the pass-B keys (pass_b_key) with shared atomics
 //            and parks every candidate's value in place; CTA r then takes bins
 //            r, r + C, ...: the maximum over the CTAs' keys and the winner's
 //            value, read from the other CTAs' shared memory (plain loads: no
@@ -26,9 +26,9 @@
 // exit keeps every CTA's shared memory alive while the others read from it.
 // Clusters of 8 or 16 CTAs of 256 threads (4096 points each, three CTAs per
 // SM) or of 4 / 8 CTAs of 512 threads (8192 points, one per SM).  Measured
-// on a B200 against the two-pass kernels (the default): 0.37 vs 0.34 us per
-// pair at n = 32768 and 0.90 vs 0.66 at 65536 on dense blocks (pass B with
-// its per-point keys takes ~45% of a CTA's time, the three barriers ~20%),
+// on a B200 against the two-pass kernels (the default): 0.35 vs 0.31 us per
+// pair at n = 32768 and 0.82 vs 0.60 at 65536 on dense blocks with binsize
+// n/16 (pass B takes ~45% of a CTA's time, the three barriers ~20%),
 // faster on short row lists at n = 32768, where the two-pass path reads the
 // row count on the host.  The arithmetic (products, FFT passes,
 // twiddles, key order) is that of large_pass_a / large_pass_b, so the outputs
@@ -86,6 +86,8 @@ cluster_kernel(const LargeArgs a) {
   const unsigned lo_mask = (1u << a.lo_bits) - 1u;
   const int bs = a.binsize;
   const float inv_bs = 1.0f / (float)bs;
+  unsigned smask = 0u, srank = 0u;
+  if (a.seg > 0) bin_segment(T1, a.seg, smask, srank);
 
   // pass-A geometry: column c of this CTA, point group t
   const int c = tid % CA, t = tid / CA;
@@ -144,11 +146,8 @@ cluster_kernel(const LargeArgs a) {
       const int k1 = t1 + T1 * q;
       const int lag = N2 * k1 + k2b;
       const float m2 = fmaf(v[q].x, v[q].x, v[q].y * v[q].y);
-      if (lag >= a.ws && lag < a.we && m2 > a.t2) {
-        const int bin = bin_of(lag - a.ws, bs, inv_bs);
-        atomicMax(keys + bin, ((unsigned long long)__float_as_uint(m2) << 32) | (unsigned)(~lag));
-        rbuf[pad16(k1)] = make_float2(v[q].x, v[q].y);
-      }
+      pass_b_key(keys, rbuf + pad16(k1), v[q], m2, lag, lag >= a.ws && lag < a.we && m2 > a.t2,
+                 a.seg, smask, srank, a.ws, bs, inv_bs);
     }
     cluster.sync();
     // ---- outputs: CTA r takes bins r, r + C, ...: maximum over the CTAs' keys -----

@@ -51,6 +51,7 @@ struct LargeArgs {
   const float2 *tw_hi, *tw_lo;          // W_n^m = tw_hi[m >> lo_bits] * tw_lo[m & lo_mask]
   int lo_bits;
   int ws, we, binsize, nb;
+  int seg;                              // pass B: threads per bin segment (bin_lanes), 0: per point
   float t2;
   long long *out_idx;
   float2 *out_val;
@@ -140,6 +141,64 @@ __device__ __forceinline__ void rec_max(uint4 *slot, uint4 mine) {
   }
 }
 
+// Pass-B keys: (|z|^2 bits with the low 5 mantissa bits cleared) << 32 | ~lag,
+// so a bin keeps its largest |z|^2 to within 2^-18 relative and, among values
+// that close, the lowest lag -- the order the single-CTA kernels use.
+//
+// Lanes of a warp that share a bin: a warp holds 32 / T1 rows k2 (T1 < 32) or
+// 32 threads of one row, thread t at k1 = t + T1 q.  With binsize = m N2 (m a
+// power of two) and the window starting on a multiple of binsize, lag
+// N2 k1 + k2 (k2 < N2) falls in bin floor(k1 / m) less a constant, so the
+// lanes sharing a bin are the aligned blocks of min(m, T1, 32) threads t of
+// every row in the warp.  Returns that block size, or 0 when the bins do not
+// line up this way or the block is shorter than 8 threads.
+__host__ __device__ inline int bin_lanes(int binsize, int ws, int N1, int N2) {
+  if (binsize % N2 != 0 || ws % binsize != 0) return 0;
+  const int m = binsize / N2;
+  if ((m & (m - 1)) != 0) return 0;
+  const int T1 = N1 / 16, cap = T1 < 32 ? T1 : 32;
+  const int seg = m < cap ? m : cap;
+  return seg >= 8 ? seg : 0;   // shorter segments: one key per point measured faster
+}
+
+// Per-thread constants of pass_b_key for T1 threads per row and seg > 0:
+// the lanes of this lane's bin segment, and its rank among them in lag order
+// (t first, then the row).
+__device__ __forceinline__ void bin_segment(int T1, int seg, unsigned &mask, unsigned &rank) {
+  const int lane = threadIdx.x & 31;
+  if (T1 >= 32) {
+    mask = seg >= 32 ? 0xffffffffu : ((1u << seg) - 1u) << (lane & ~(seg - 1));
+    rank = (unsigned)lane;
+  } else {
+    const int rows = 32 / T1, t = lane % T1, row = lane / T1;
+    const unsigned block = ((1u << seg) - 1u) << (t & ~(seg - 1));
+    mask = 0u;
+    for (int r = 0; r < rows; r++) mask |= block << (r * T1);
+    rank = (unsigned)(t * rows + row);
+  }
+}
+
+// One step of pass B: this thread's z = v at `lag` (a candidate when `cand`).
+// With seg > 0 the warp first reduces each bin segment (one redux; the winner,
+// unique by rank, parks its value and publishes the segment's key); otherwise
+// every candidate parks and publishes.  `park` is where the value goes.
+__device__ __forceinline__ void pass_b_key(unsigned long long *keys, float2 *park, cf v, float m2,
+                                           int lag, bool cand, int seg, unsigned mask,
+                                           unsigned rank, int ws, int bs, float inv_bs) {
+  const unsigned mt = __float_as_uint(m2) & ~31u;
+  if (seg > 0) {
+    const unsigned k32 = cand ? (mt | (31u - rank)) : 0u;
+    const unsigned mx = __reduce_max_sync(mask, k32);
+    if (k32 != 0u && k32 == mx) {
+      *park = make_float2(v.x, v.y);
+      atomicMax(keys + bin_of(lag - ws, bs, inv_bs), ((unsigned long long)mt << 32) | (unsigned)(~lag));
+    }
+  } else if (cand) {
+    *park = make_float2(v.x, v.y);
+    atomicMax(keys + bin_of(lag - ws, bs, inv_bs), ((unsigned long long)mt << 32) | (unsigned)(~lag));
+  }
+}
+
 template <int N1>
 __global__ void __launch_bounds__(FlatGeo<N1>::CTA)
 large_pass_b(const LargeArgs a) {
@@ -151,6 +210,8 @@ large_pass_b(const LargeArgs a) {
   unsigned long long *keys = reinterpret_cast<unsigned long long *>(smem + G * Geo::BUF);
   const int bs = a.binsize;
   const float inv_bs = 1.0f / (float)bs;
+  unsigned smask = 0u, srank = 0u;
+  if (a.seg > 0) bin_segment(T1, a.seg, smask, srank);
   const long long work = (long long)a.batch * a.N2 / G;
   for (long long w = blockIdx.x; w < work; w += gridDim.x) {
     const long long r0 = w * G;                       // first row of this CTA
@@ -173,11 +234,9 @@ large_pass_b(const LargeArgs a) {
       const int k1 = t + T1 * q;
       const int lag = a.N2 * k1 + k2;
       const float m2 = fmaf(v[q].x, v[q].x, v[q].y * v[q].y);
-      if (live && lag >= a.ws && lag < a.we && m2 > a.t2) {
-        const int bin = bin_of(lag - a.ws, bs, inv_bs);
-        atomicMax(keys + bin, ((unsigned long long)__float_as_uint(m2) << 32) | (unsigned)(~lag));
-        buf[pad16(k1)] = make_float2(v[q].x, v[q].y);
-      }
+      pass_b_key(keys, buf + pad16(k1), v[q], m2, lag,
+                 live && lag >= a.ws && lag < a.we && m2 > a.t2, a.seg, smask, srank, a.ws, bs,
+                 inv_bs);
     }
     __syncthreads();
     for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {

@@ -644,6 +644,7 @@ static int run_large(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t 
   a.ws = (int)start; a.we = (int)end;
   a.binsize = binsize > p->n ? (int)p->n : (int)binsize;
   a.nb = (int)nb;
+  a.seg = bin_lanes(a.binsize, a.ws, c.N1, c.N2);
   a.t2 = threshold > 0.f ? threshold * threshold : 0.f;
   a.out_idx = (long long *)idx;
   a.out_val = (float2 *)val;
