@@ -83,7 +83,6 @@ cluster_kernel(const LargeArgs a) {
   const int cid = (int)(blockIdx.x / C);
   const int tid = threadIdx.x;
   const long long total = a.list_count ? (long long)(*a.list_count) : a.total;
-  const unsigned lo_mask = (1u << a.lo_bits) - 1u;
   const int bs = a.binsize;
   const float inv_bs = 1.0f / (float)bs;
   unsigned smask = 0u, srank = 0u;
@@ -115,13 +114,7 @@ cluster_kernel(const LargeArgs a) {
       }
     }
     inverse_passes<N2, true>(v, cbuf, a.tw2, t);
-#pragma unroll
-    for (int q = 0; q < 16; q++) {
-      const int k2 = t + T2 * q;
-      const unsigned m = ((unsigned)f1 * (unsigned)k2) & (unsigned)(a.n - 1);
-      const float2 wh = __ldg(a.tw_hi + (m >> a.lo_bits)), wl = __ldg(a.tw_lo + (m & lo_mask));
-      v[q] = cmul(v[q], cmul(cf{wh.x, wh.y}, cf{wl.x, wl.y}));
-    }
+    pass_a_twiddle<T2>(v, a, f1, t);
     // every CTA has read the previous pair's keys and parked values (the
     // values read were consumed before this barrier: no release needed)
     cluster_sync_relaxed();

@@ -73,6 +73,30 @@ __device__ __forceinline__ void large_pair(const LargeArgs &a, long long pi, int
   }
 }
 
+// W_n^m from the two-level table (FP64-built halves, one product).
+__device__ __forceinline__ cf wn_table(const LargeArgs &a, unsigned m) {
+  const float2 wh = __ldg(a.tw_hi + (m >> a.lo_bits));
+  const float2 wl = __ldg(a.tw_lo + (m & ((1u << a.lo_bits) - 1u)));
+  return cmul(cf{wh.x, wh.y}, cf{wl.x, wl.y});
+}
+
+// Pass A's twiddle: v[q] *= W_n^(f1 k2), k2 = t + T2 q.  The factor comes
+// from the table at q = 0, 4, 8, 12 and from up to three steps of
+// W_n^(f1 T2) in between (10 table reads instead of 32; the three products
+// add at most a few float ulps).
+template <int T2>
+__device__ __forceinline__ void pass_a_twiddle(cf *v, const LargeArgs &a, int f1, int t) {
+  const unsigned nm = (unsigned)(a.n - 1);
+  const cf step = wn_table(a, ((unsigned)f1 * (unsigned)T2) & nm);
+  cf w;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    if ((q & 3) == 0) w = wn_table(a, ((unsigned)f1 * (unsigned)(t + T2 * q)) & nm);
+    else w = cmul(w, step);
+    v[q] = cmul(v[q], w);
+  }
+}
+
 template <int N2>
 __global__ void __launch_bounds__(N2 >= 256 ? N2 : 256, N2 >= 1024 ? 1 : (N2 >= 512 ? 2 : 3))
 large_pass_a(const LargeArgs a) {
@@ -83,7 +107,6 @@ large_pass_a(const LargeArgs a) {
   float2 *buf = smem + c * col_buf<N2>();
   const int tiles = a.N1 / C;
   const long long work = (long long)a.batch * tiles;
-  const unsigned lo_mask = (1u << a.lo_bits) - 1u;
   for (long long w = blockIdx.x; w < work; w += gridDim.x) {
     const int bp = (int)(w / tiles), tile = (int)(w - (long long)bp * tiles);
     const long long pi = a.pair0 + bp;
@@ -106,16 +129,11 @@ large_pass_a(const LargeArgs a) {
       for (int s = 0; s < 16; s++) v[s] = {0.f, 0.f};
     }
     inverse_passes<N2, true>(v, buf, a.tw2, t);
+    pass_a_twiddle<T2>(v, a, f1, t);
     float2 *yp = a.Y + (long long)bp * a.N2 * a.N1 + f1;
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-      const int k2 = t + T2 * q;
-      const unsigned m = ((unsigned)f1 * (unsigned)k2) & (unsigned)(a.n - 1);
-      const float2 wh = __ldg(a.tw_hi + (m >> a.lo_bits)), wl = __ldg(a.tw_lo + (m & lo_mask));
-      const cf tw = cmul(cf{wh.x, wh.y}, cf{wl.x, wl.y});
-      const cf y = cmul(v[q], tw);
-      yp[(long long)k2 * a.N1] = make_float2(y.x, y.y);
-    }
+    for (int q = 0; q < 16; q++)
+      yp[(long long)(t + T2 * q) * a.N1] = make_float2(v[q].x, v[q].y);
   }
 }
 
@@ -213,6 +231,11 @@ large_pass_b(const LargeArgs a) {
   unsigned smask = 0u, srank = 0u;
   if (a.seg > 0) bin_segment(T1, a.seg, smask, srank);
   const long long work = (long long)a.batch * a.N2 / G;
+  // With at most one bin per thread, a thread's merge into the records waits
+  // until its next rows' loads are in flight (its L2 round trip overlaps them).
+  const bool defer = a.nb <= (int)blockDim.x;
+  uint4 pend = make_uint4(0u, 0u, 0u, 0u);
+  uint4 *pend_at = nullptr;
   for (long long w = blockIdx.x; w < work; w += gridDim.x) {
     const long long r0 = w * G;                       // first row of this CTA
     const int bp = (int)(r0 / a.N2), k2base = (int)(r0 - (long long)bp * a.N2);
@@ -224,6 +247,10 @@ large_pass_b(const LargeArgs a) {
     for (int s = 0; s < 16; s++) {
       const float2 x = yp[t + T1 * s];
       v[s] = {x.x, x.y};
+    }
+    if (pend_at) {
+      rec_max(pend_at, pend);
+      pend_at = nullptr;
     }
     for (int b = threadIdx.x; b < a.nb; b += blockDim.x) keys[b] = 0ull;
     __syncthreads();
@@ -245,12 +272,18 @@ large_pass_b(const LargeArgs a) {
       const int lag = (int)(~(unsigned)kk);
       const int gw = (lag % a.N2) - k2base, k1w = lag / a.N2;
       const float2 val = smem[gw * Geo::BUF + pad16(k1w)];
-      rec_max(a.rec + (long long)bp * a.nb + b,
-              make_uint4(__float_as_uint(val.x), __float_as_uint(val.y), (unsigned)kk,
-                         (unsigned)(kk >> 32)));
+      const uint4 r = make_uint4(__float_as_uint(val.x), __float_as_uint(val.y), (unsigned)kk,
+                                 (unsigned)(kk >> 32));
+      if (defer) {
+        pend = r;
+        pend_at = a.rec + (long long)bp * a.nb + b;
+      } else {
+        rec_max(a.rec + (long long)bp * a.nb + b, r);
+      }
     }
     __syncthreads();
   }
+  if (pend_at) rec_max(pend_at, pend);
 }
 
 // Forward transforms of series blocks for n > 16384 (run_series): the same

@@ -497,6 +497,7 @@ extern "C" int mfb_create(mfb_plan **out, size_t n, int ndata, int ntmpl, int de
   mfb_plan *p = new mfb_plan;
   p->device = device;
   p->n = n;
+  p->cluster = n == 32768 ? 1 : 0;   // the faster kernel at each length (mfb_set_cluster)
   p->nd = ndata;
   p->nt = ntmpl;
   int r = is_large(n) ? get_large(device, (int)n, &p->lc) : get_const(device, (int)n, &p->c);

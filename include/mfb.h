@@ -88,16 +88,17 @@ int mfb_run_records(mfb_plan *p, int d0, int nd, int t0, int nt, size_t binsize,
 int mfb_set_packed(mfb_plan *p, int on);
 /* Kernel choice for n = 32768 and 65536 (no counterpart in the reference,
    whose CPU engine always runs its four-step plan through memory): mode 0
-   (the default) runs the two-pass kernels through the plan's L2-sized
-   scratch; mode 1 runs each pair on one thread-block cluster whose
-   distributed shared memory holds the whole spectrum between the two passes
-   of the four-step split -- 8 (n = 32768) or 16 (n = 65536) CTAs of 256
-   threads, three CTAs per SM -- in one launch with no scratch and no host
-   decision (listed runs read their row count on the device, so a
-   hierarchical run at these lengths is replayed as one CUDA graph); mode 2
-   the same with 4 / 8 CTAs of 512 threads, one per SM.  Same arithmetic,
-   identical results.  On a B200 the cluster kernels measure 1.1-1.4x slower
-   than mode 0 on dense blocks and faster on short lists at n = 32768. */
+   runs the two-pass kernels through the plan's L2-sized scratch; mode 1 runs
+   each pair on one thread-block cluster whose distributed shared memory
+   holds the whole spectrum between the two passes of the four-step split --
+   8 (n = 32768) or 16 (n = 65536) CTAs of 256 threads, three CTAs per SM --
+   in one launch with no scratch and no host decision (listed runs read their
+   row count on the device, so a hierarchical run at these lengths is
+   replayed as one CUDA graph); mode 2 the same with 4 / 8 CTAs of 512
+   threads, one per SM.  Same arithmetic, identical results.  The default is
+   the faster on a B200: mode 1 at n = 32768 (on a par with mode 0 on dense
+   blocks, faster on short row lists), mode 0 at 65536 (mode 1 is 1.3x
+   slower there). */
 int mfb_set_cluster(mfb_plan *p, int mode);
 /* Replaces ap_mf_run_sel (src/matchfilt.c:492-503) in list form: run only the
    output rows rows[0..*nrows) of the block [d0,d0+nd) x [t0,t0+nt), where a row
