@@ -168,15 +168,14 @@ __device__ __forceinline__ void rec_max(uint4 *slot, uint4 mine) {
 // power of two) and the window starting on a multiple of binsize, lag
 // N2 k1 + k2 (k2 < N2) falls in bin floor(k1 / m) less a constant, so the
 // lanes sharing a bin are the aligned blocks of min(m, T1, 32) threads t of
-// every row in the warp.  Returns that block size, or 0 when the bins do not
-// line up this way or the block is shorter than 8 threads.
+// every row in the warp.  Returns that block size when it spans the warp
+// (every lane of a warp then shares one bin), else 0.
 __host__ __device__ inline int bin_lanes(int binsize, int ws, int N1, int N2) {
   if (binsize % N2 != 0 || ws % binsize != 0) return 0;
   const int m = binsize / N2;
   if ((m & (m - 1)) != 0) return 0;
   const int T1 = N1 / 16, cap = T1 < 32 ? T1 : 32;
-  const int seg = m < cap ? m : cap;
-  return seg >= 8 ? seg : 0;   // shorter segments: one key per point measured faster
+  return m >= cap ? cap : 0;   // whole-warp segments only: several per warp measured slower
 }
 
 // Per-thread constants of pass_b_key for T1 threads per row and seg > 0:
@@ -205,6 +204,7 @@ __device__ __forceinline__ void pass_b_key(unsigned long long *keys, float2 *par
                                            unsigned rank, int ws, int bs, float inv_bs) {
   const unsigned mt = __float_as_uint(m2) & ~31u;
   if (seg > 0) {
+    if (!__any_sync(mask, cand)) return;   // the usual case above a threshold
     const unsigned k32 = cand ? (mt | (31u - rank)) : 0u;
     const unsigned mx = __reduce_max_sync(mask, k32);
     if (k32 != 0u && k32 == mx) {
@@ -218,7 +218,7 @@ __device__ __forceinline__ void pass_b_key(unsigned long long *keys, float2 *par
 }
 
 template <int N1>
-__global__ void __launch_bounds__(FlatGeo<N1>::CTA)
+__global__ void __launch_bounds__(FlatGeo<N1>::CTA, 4)   // 64 registers: four CTAs per SM
 large_pass_b(const LargeArgs a) {
   using Geo = FlatGeo<N1>;
   constexpr int T1 = Geo::T, G = Geo::G;
@@ -231,11 +231,6 @@ large_pass_b(const LargeArgs a) {
   unsigned smask = 0u, srank = 0u;
   if (a.seg > 0) bin_segment(T1, a.seg, smask, srank);
   const long long work = (long long)a.batch * a.N2 / G;
-  // With at most one bin per thread, a thread's merge into the records waits
-  // until its next rows' loads are in flight (its L2 round trip overlaps them).
-  const bool defer = a.nb <= (int)blockDim.x;
-  uint4 pend = make_uint4(0u, 0u, 0u, 0u);
-  uint4 *pend_at = nullptr;
   for (long long w = blockIdx.x; w < work; w += gridDim.x) {
     const long long r0 = w * G;                       // first row of this CTA
     const int bp = (int)(r0 / a.N2), k2base = (int)(r0 - (long long)bp * a.N2);
@@ -247,10 +242,6 @@ large_pass_b(const LargeArgs a) {
     for (int s = 0; s < 16; s++) {
       const float2 x = yp[t + T1 * s];
       v[s] = {x.x, x.y};
-    }
-    if (pend_at) {
-      rec_max(pend_at, pend);
-      pend_at = nullptr;
     }
     for (int b = threadIdx.x; b < a.nb; b += blockDim.x) keys[b] = 0ull;
     __syncthreads();
@@ -272,18 +263,12 @@ large_pass_b(const LargeArgs a) {
       const int lag = (int)(~(unsigned)kk);
       const int gw = (lag % a.N2) - k2base, k1w = lag / a.N2;
       const float2 val = smem[gw * Geo::BUF + pad16(k1w)];
-      const uint4 r = make_uint4(__float_as_uint(val.x), __float_as_uint(val.y), (unsigned)kk,
-                                 (unsigned)(kk >> 32));
-      if (defer) {
-        pend = r;
-        pend_at = a.rec + (long long)bp * a.nb + b;
-      } else {
-        rec_max(a.rec + (long long)bp * a.nb + b, r);
-      }
+      rec_max(a.rec + (long long)bp * a.nb + b,
+              make_uint4(__float_as_uint(val.x), __float_as_uint(val.y), (unsigned)kk,
+                         (unsigned)(kk >> 32)));
     }
     __syncthreads();
   }
-  if (pend_at) rec_max(pend_at, pend);
 }
 
 // Forward transforms of series blocks for n > 16384 (run_series): the same
