@@ -46,7 +46,9 @@ def test_cluster_equals_two_pass_and_oracle(n):
     for binsize, thr, win in [(n // 16, 0.0, None), (n // 64, 0.0, None),
                               (n // 100 + 7, 0.0, (13, n - 5)),
                               (n // 8, 5.0 * np.sqrt(n), (n // 3, n)), (n, 0.0, None),
-                              (1000, 0.0, (n // 2 - 20000, n // 2 + 20000))]:
+                              (1000, 0.0, (n // 2 - 20000, n // 2 + 20000)),
+                              (n // 16, 0.0, (n // 16, n)),        # window on a bin edge
+                              (16, 0.0, None)]:                    # 2048 / 4096 bins
         (a, ca), (a2, ca2), (b, cb) = _modes(f, binsize=binsize, threshold=thr, window=win)
         for x, cx in ((a, ca), (a2, ca2)):
             np.testing.assert_array_equal(x["index"], b["index"])

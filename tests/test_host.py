@@ -125,3 +125,18 @@ def test_large_workload_subsample_is_the_full_banks_draws():
     torch.testing.assert_close(H1[[2, 7, 11]], H2)
     assert np.isclose(float(p1.sum()) * n / n, float((H1.abs().double() ** 2).mean(0).sum()),
                       rtol=1e-6)
+
+
+def test_repeat_key_accepts_only_immutable_arguments():
+    """run() arguments that a later call can be compared with by value (None,
+    numbers, tuples of ints) identify a repeat; lists, arrays and NaN do not."""
+    import numpy as np
+    from apogee_b200 import _repeat_key
+    assert _repeat_key(256, 5.5, None, None, None) == (256, 5.5, None, None, None)
+    assert _repeat_key(None, 0, (0, 4096), (0, 16), (8, 64)) is not None
+    assert _repeat_key(256, 5.5, [0, 4096], None, None) is None
+    assert _repeat_key(256, 5.5, np.array([0, 4096]), None, None) is None
+    assert _repeat_key(256, float("nan"), None, None, None) is None
+    assert _repeat_key(np.int64(256), 5.5, None, None, None) is None
+    assert _repeat_key(256, np.float32(5.5), None, None, None) is None
+    assert _repeat_key(256, 5.5, (0, 4096.0), None, None) is None
