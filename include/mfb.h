@@ -103,7 +103,11 @@ int mfb_set_cluster(mfb_plan *p, int mode);
 /* Replaces ap_mf_run_sel (src/matchfilt.c:492-503) in list form: run only the
    output rows rows[0..*nrows) of the block [d0,d0+nd) x [t0,t0+nt), where a row
    is (d-d0)*nt + (t-t0) and the row count lives in DEVICE memory (nrows), so a
-   survivor list made on the GPU needs no host round trip.  max_rows bounds it. */
+   survivor list made on the GPU needs no host round trip.  The caller keeps
+   *nrows <= max_rows.  Every kernel reads the count on the device, except the
+   two-pass kernels (n >= 65536, and n = 32768 in cluster mode 0), which size
+   their batches on the host: there the call reads the count, synchronises the
+   plan's stream and refuses a count above max_rows. */
 int mfb_run_rows(mfb_plan *p, int d0, int nd, int t0, int nt, const int32_t *rows,
                  const int32_t *nrows, int max_rows, size_t binsize, float threshold,
                  size_t start, size_t end, int64_t *idx, void *val, int32_t *counts);
