@@ -113,6 +113,14 @@ __device__ __forceinline__ void tc_after_sync() {
                  "=r"(r[30]), "=r"(r[31])                                                          \
                : "r"(taddr))
 
+#define MFB_TMEM_LD16(taddr, r)                                                                    \
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "                                            \
+               "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"                     \
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),          \
+                 "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),        \
+                 "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])                                \
+               : "r"(taddr))
+
 __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -343,21 +351,24 @@ coarse_tc_ws_kernel(const TcKernelArgs a) {
       const uint32_t u = (uint32_t)(it / NSLOT);
       mbar_wait_ab(bar(tcw::B_FULL1 + k), u & 1, abort_flag, a.err);                       // S1[k] full
       tc_after_sync();
-      uint32_t v0[32], v1[32];
-      MFB_TMEM_LD32(tmem + ((uint32_t)(32 * q) << 16) + k * 64, v0);
-      MFB_TMEM_LD32(tmem + ((uint32_t)(32 * q) << 16) + k * 64 + 32, v1);
-      tmem_wait_ld();
-      tc_before_sync();
-      if (lane == 0) mbar_arrive(bar(tcw::B_FREE1 + k));
+      uint32_t vv[16];
       if (it >= NSLOT) mbar_wait_ab(bar(tcw::B_FULL2 + k), (u - 1) & 1, abort_flag, a.err);  // A2[k] consumed
       uint8_t *a2 = sm + tcw::OFF_A2 + k * tcw::SLOT;
 #pragma unroll
-      for (int s = 0; s < 2; s++) {
-        const int p = 4 * s + q;
+      for (int hh = 0; hh < 4; hh++) {
+        // 16 accumulator columns (8 values j1 of one tile) at a time: few
+        // registers live, so the compiler can overlap the elements' chains
+        const int s = hh >> 1, p = 4 * s + q;
+        MFB_TMEM_LD16(tmem + ((uint32_t)(32 * q) << 16) + k * 64 + 16 * hh, vv);
+        tmem_wait_ld();
+        if (hh == 3) {   // both tiles read: S1[k] is free
+          tc_before_sync();
+          if (lane == 0) mbar_arrive(bar(tcw::B_FREE1 + k));
+        }
 #pragma unroll
-        for (int j1 = 0; j1 < 16; j1++) {
-          const uint32_t *vv = s ? v1 : v0;
-          const float yr = __uint_as_float(vv[2 * j1]), yi = __uint_as_float(vv[2 * j1 + 1]);
+        for (int jj = 0; jj < 8; jj++) {
+          const int j1 = 8 * (hh & 1) + jj;
+          const float yr = __uint_as_float(vv[2 * jj]), yi = __uint_as_float(vv[2 * jj + 1]);
           const float2 w = tw[j1];
           const float zr = fmaf(yr, w.x, -yi * w.y), zi = fmaf(yr, w.y, yi * w.x);
           uint32_t hi, lo;
