@@ -20,8 +20,8 @@
 //    values as the scalar tables, duplicated for the two lanes; six of the
 //    fifteen per pass are read, the others are products of two of those
 //    (pass_twiddles), which halves the kernel's L1 traffic for twiddles at
-//    the cost of about one float ulp in nine of them (the kernel is then no
-//    longer bit-identical to the scalar one; both meet the oracle's bar).
+//    the cost of about one float ulp in nine of them; the one-pair kernels
+//    form theirs the same way, so the outputs stay bit-identical.
 // Scope: n = 4096, MODE_PEAKS, the whole lag window with bins a multiple of
 // 32 lags and at most KEYCAP bins (the benchmark's and the refine's layout);
 // the launcher sends every other run to flat_kernel / rows_kernel.

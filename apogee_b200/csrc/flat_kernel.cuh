@@ -129,6 +129,35 @@ __device__ __forceinline__ void pass_sync(int T) {
   if constexpr (CTA_SYNC) __syncthreads(); else group_sync(T);
 }
 
+// v[q] *= w^q, q = 1..15, for one radix-16 pass: w^1, w^2, w^3, w^4, w^8 and
+// w^12 come from the FP64-built table (entry q at tw[(q-1)*stride]), the other
+// nine are one product of two of those (w^(4a+b) = w^(4a) w^b), a rounding
+// error of about one float ulp beside the table's half ulp.  The packed
+// two-pair kernel forms its twiddles with the same operations in the same
+// order, so the two kernels give bit-identical outputs.
+__device__ __forceinline__ void pass_twiddles(cf *v, const float2 *tw, int stride) {
+  auto ld = [&](int q) {
+    const float2 w = __ldg(tw + (q - 1) * stride);
+    return cf{w.x, w.y};
+  };
+  const cf w1 = ld(1), w2 = ld(2), w3 = ld(3), w4 = ld(4), w8 = ld(8), w12 = ld(12);
+  v[1] = cmul(v[1], w1);
+  v[2] = cmul(v[2], w2);
+  v[3] = cmul(v[3], w3);
+  v[4] = cmul(v[4], w4);
+  v[5] = cmul(v[5], cmul(w4, w1));
+  v[6] = cmul(v[6], cmul(w4, w2));
+  v[7] = cmul(v[7], cmul(w4, w3));
+  v[8] = cmul(v[8], w8);
+  v[9] = cmul(v[9], cmul(w8, w1));
+  v[10] = cmul(v[10], cmul(w8, w2));
+  v[11] = cmul(v[11], cmul(w8, w3));
+  v[12] = cmul(v[12], w12);
+  v[13] = cmul(v[13], cmul(w12, w1));
+  v[14] = cmul(v[14], cmul(w12, w2));
+  v[15] = cmul(v[15], cmul(w12, w3));
+}
+
 // Unnormalised inverse FFT of the n values x[t + T*s] = v[s] held by the T
 // threads of one pair slot (Stockham autosort: pass 0 radix R0, then radix
 // 16).  On return v[q] = X[t + T*q].  buf is this slot's padded shared buffer;
@@ -187,12 +216,7 @@ __device__ __forceinline__ void inverse_passes(cf *v, float2 *buf, const float2 
       }
     }
     const int k = t & (Ns - 1);
-    const float2 *tw = twid + twiddle_offset<N>(p) + k;
-#pragma unroll
-    for (int q = 1; q < 16; q++) {
-      const float2 w = __ldg(tw + (q - 1) * Ns);
-      v[q] = cmul(v[q], cf{w.x, w.y});
-    }
+    pass_twiddles(v, twid + twiddle_offset<N>(p) + k, Ns);
     dftR<16, 0, 1>(v);
     pass_sync<CTA_SYNC>(T);
     if (p < PASSES - 1) {

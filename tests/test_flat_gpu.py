@@ -304,9 +304,9 @@ def _same_up_to_near_ties(i1, i2, z):
 def test_packed_kernel_matches_one_pair_kernel_and_oracle(nd, nt, binsize, threshold):
     """n = 4096 runs over the whole window use the kernel that carries two
     pairs per thread in packed FP32x2 arithmetic.  It must meet the oracle's
-    bar and agree with the one-pair kernel (dense, listed and record output,
-    counts), indices up to FP64 near-ties; listed rows equal the dense run's
-    rows bit for bit."""
+    bar and equal the one-pair kernel bit for bit (dense, listed and record
+    output, counts: both form their twiddles with the same operations); listed
+    rows equal the dense run's rows bit for bit."""
     import torch
     import apogee_b200 as mf
     from apogee_b200 import _lib
@@ -334,6 +334,8 @@ def test_packed_kernel_matches_one_pair_kernel_and_oracle(nd, nt, binsize, thres
             bad = parity.compare(r["index"], r["value"], z, binsize, threshold)
             assert not bad, (packed, bad[:3])
         _same_up_to_near_ties(out[0][2][:, t0:t0 + 128], out[1][2][:, t0:t0 + 128], z)
+    np.testing.assert_array_equal(out[0][2], out[1][2])
+    np.testing.assert_array_equal(out[0][3], out[1][3])
     # listed rows in arbitrary order, an odd count
     rows = np.random.default_rng(7).permutation(nd * nt)[: max(1, (nd * nt) // 2) | 1]
     rows_d = torch.as_tensor(rows.astype(np.int32), device="cuda")
