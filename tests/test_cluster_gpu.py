@@ -137,3 +137,18 @@ def test_cluster_hierarchical_refine_and_host_table():
         np.testing.assert_array_equal(ridx, oidx)
         np.testing.assert_array_equal(rval, oval)
         assert tab["index"][step % nd, t, lag // (n // 16)] == lag
+
+
+def test_cluster_mode_argument_checked():
+    """Modes 0, 1 and 2 are accepted at any length (they select nothing below
+    n = 32768); anything else is an argument error."""
+    import apogee_b200 as mf
+    from apogee_b200 import _lib
+    L = _lib.lib()
+    for n in (4096, 32768):
+        f = mf.MatchedFilter(n, 1, 1)
+        for mode in (0, 1, 2):
+            assert L.mfb_set_cluster(f._plan, mode) == 0
+        for mode in (-1, 3):
+            assert L.mfb_set_cluster(f._plan, mode) == _lib.MFB_ERR_ARG
+            assert "cluster mode" in L.mfb_last_error().decode()
